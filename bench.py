@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Throughput of the CUMC3D per-step hot path on B200.
+
+Workload: 3-D Orszag-Tang vortex, 256^3 cells, FP64, PPM + HLL + CT + SSP-RK3
+at CFL 0.4 (the throughput configuration). One step = one full main-loop
+iteration of solver/main.f90:127-143: finddt, then the three RK stages.
+Metric: Mcell-upd/s = cells * steps / seconds / 1e6, whole job (all ranks).
+
+  python bench.py [--gpus N --steps K --warmup W]      this library
+  python bench.py --impl reference ...                  the FP64 CPU restatement
+                                                        of the reference, all host
+                                                        threads (rank 0 only)
+
+N > 1 runs independent replicas, one per GPU (the hot path is one domain on
+one GPU; there is no data-path collective); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-upd/s @256^3 (FP64, Orszag-Tang 3D, PPM/HLL/CT/RK3)"
+UNIT = "Mcell-upd/s"
+BYTES_PER_CELL_UPDATE = 512  # algorithmic HBM bytes of one cell through one RK3 step (FP64)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dram_traffic_table():
+    """per-launch DRAM bytes of each kernel at the bench workload, from the
+    committed ncu summary (profiles/dram_traffic_orszag_tang_256.txt)."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_orszag_tang_256.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 2 and not line.startswith("#"):
+                try:
+                    out[parts[0]] = float(parts[1])
+                except ValueError:
+                    pass
+    return out
+
+
+def algorithmic_bytes(kernel: str, nx: int, ny: int, nz: int) -> float:
+    """compulsory HBM bytes of one launch (each value read or written once)."""
+    n = (nx, ny, nz)
+    if kernel.startswith("sweep_"):
+        d = "xyz".index(kernel[-1])
+        t = [n[a] + 2 for a in range(3) if a != d]
+        faces = (n[d] + 1) * t[0] * t[1]
+        cells = (n[d] + 6) * t[0] * t[1]
+        return 8.0 * (7 * cells + faces + 7 * faces)
+    box1 = (nx + 1) * (ny + 1) * (nz + 1)
+    box2 = (nx + 2) * (ny + 2) * (nz + 2)
+    if kernel == "emf":
+        return 8.0 * (6 * box2 + 6 * box2 + 3 * box1)
+    if kernel == "combine":  # 15 hydro fluxes + 3 EMF + u0 + uc + result (stage 2/3 form)
+        return 8.0 * (15 + 3 + 8 + 8 + 8) * box1
+    if kernel == "utop":
+        return 8.0 * (8 + 2 + 5 + 5 + 1 + 3) * box1
+    if kernel == "boundary":
+        ghosts = (nx + 6) * (ny + 6) * (nz + 6) - nx * ny * nz
+        return 8.0 * 2 * 12 * ghosts
+    if kernel == "finddt":
+        return 8.0 * 8 * nx * ny * nz
+    return float("nan")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.6)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append({"sm": float(p[1]), "max": float(p[2]), "power": float(p[3]), "hw": p[5], "hwt": p[6],
+                             "swt": p[7], "pcap": p[8]})
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        load = [r for r in rows if r["power"] > 250.0] or rows
+        reasons = set()
+        for r in load:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                              ("pcap", "sw_power_cap")):
+                if r[key].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in load), "sm_max_mhz": max(r["max"] for r in rows),
+                "samples": len(load), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(n: int, nz: int, steps: int, warmup: int, threads: int | None = None):
+    """FP64 CPU restatement on an Orszag-Tang slab of n x n x nz cells at the
+    bench resolution (cell size 1/n); returns (Mcell-upd/s, threads, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from cumpic_b200 import problems as P
+    from _oracle import Oracle, lib as oracle_lib
+
+    threads = threads or os.cpu_count() or 1
+    p = P.orszag_tang(n, nz=nz)
+    o = Oracle(p, threads=threads)
+    used = oracle_lib().orc_get_threads()
+    o.upload()
+    o.initial_update()
+    for _ in range(warmup):
+        o.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step()
+    el = time.perf_counter() - t0
+    return p.cells * steps / el / 1e6, used, el
+
+
+def calibrate_slab(n: int, seconds_per_step: float, threads: int | None = None) -> int:
+    rate, _, _ = cpu_reference_rate(32, 32, 1, 1, threads)  # Mcell-upd/s at a small size
+    nz = int(rate * 1e6 * seconds_per_step / (n * n))
+    return max(4, min(n, nz))
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    n = args.n
+    budget = 150.0  # seconds for warmup + steps
+    nz = calibrate_slab(n, budget / max(1, args.steps + args.warmup))
+    rate, threads, el = cpu_reference_rate(n, nz, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"orszag_tang_3d n={n} fp64 ppm/hll/ct/rk3", "sample": f"{n}x{n}x{nz} slab, cell size 1/{n}"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"Orszag-Tang {n}x{n}x{nz} slab at cell size 1/{n}, {args.steps} RK3 steps "
+                                   f"after {args.warmup} warm-up (FP64 C++ restatement, OpenMP)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+    import numpy as np
+
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    from cumpic_b200 import problems as P
+    from cumpic_b200.solver import CUMC3D
+
+    n = args.n
+    prob = P.orszag_tang(n)
+    cells = prob.cells
+    sim = CUMC3D(prob)
+    sim.upload()
+    sim.initial_update()
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    sim.advance(args.warmup)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- timed region: K main-loop steps, inputs resident in HBM ----------
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    sim.profile(True)
+    l0 = sim.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.advance(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = sim.launch_count() - l0
+    prof = sim.profile_read()
+    sim.profile(False)
+    barrier()
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms)
+    value = world * cells * args.steps / (ms_max / 1e3) / 1e6
+
+    # ---- roofline of the dominant kernel ------------------------------------
+    hbm, hbm_kind = peaks()
+    dom = max(prof, key=lambda k: prof[k][1])
+    dom_n, dom_ms = prof[dom]
+    per_launch_s = dom_ms / dom_n / 1e3
+    alg = algorithmic_bytes(dom, prob.nx, prob.ny, prob.nz)
+    achieved = alg / per_launch_s / 1e9
+    traffic = dram_traffic_table().get(dom)
+    kernels = {k: {"launches": v[0], "ms": round(v[1], 3), "share": round(v[1] / max(1e-9, sum(x[1] for x in prof.values())), 4)}
+               for k, v in prof.items()}
+    step_s = ms_max / 1e3 / args.steps
+    step_achieved = BYTES_PER_CELL_UPDATE * cells / step_s / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"orszag_tang_3d n={n} fp64 ppm/hll/ct/rk3 cfl=0.4",
+                   "cells_per_gpu": cells, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (each of the 8 state arrays is %.2f GB)" % (8 * (n + 6) ** 3 / 1e9)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "peak_kind": hbm_kind,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_s * 1e3,
+                     "step": {"bytes_per_cell_update": BYTES_PER_CELL_UPDATE, "achieved": step_achieved,
+                              "frac": step_achieved / hbm}},
+        "kernels": kernels,
+        "clocks": clk,
+    }
+
+    # ---- end to end through the C-ABI with host buffers ----------------------
+    if not args.no_e2e:
+        nz6, ny6, nx6 = prob.nz + 6, prob.ny + 6, prob.nx + 6
+        hp = torch.empty((nz6, ny6, nx6, 8), dtype=torch.float64, pin_memory=True).numpy()
+        he = torch.empty((nz6, ny6, nx6), dtype=torch.float64, pin_memory=True).numpy()
+        hp[...] = prob.prim
+        he[...] = prob.eps
+        out = {k: torch.empty(s, dtype=torch.float64, pin_memory=True).numpy() for k, s in
+               (("prim", (nz6, ny6, nx6, 8)), ("cons", (nz6, ny6, nx6, 8)), ("eps", (nz6, ny6, nx6)),
+                ("bcell", (nz6, ny6, nx6, 3)))}
+        sim2 = CUMC3D(prob)
+        s2 = torch.cuda.ExternalStream(sim2.stream_handle())
+        sim2.upload(hp, he)
+        sim2.initial_update()
+        sim2.step()  # warm-up of the host loop path
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        f0.record(s2)
+        sim2.upload(hp, he)
+        sim2.initial_update()
+        for _ in range(args.steps):
+            sim2.step()  # finddt -> dt to host -> clip -> rungekutta(dt)
+        from cumpic_b200.solver import _dp
+        lib = sim2._lib
+        sim2._check(lib.cumc_download_state(sim2._h, _dp(out["prim"]), _dp(out["cons"]), _dp(out["eps"]),
+                                            _dp(out["bcell"])))
+        f1.record(s2)
+        f1.synchronize()
+        wall = time.perf_counter() - t0
+        e_ms = max_over_ranks(max(f0.elapsed_time(f1), 1e3 * wall))
+        state_in = hp.nbytes + he.nbytes
+        state_out = sum(a.nbytes for a in out.values())
+        line["e2e"] = {"value": world * cells * args.steps / (e_ms / 1e3) / 1e6, "unit": UNIT,
+                       "h2d_bytes_per_step": int(state_in / args.steps + 8),
+                       "d2h_bytes_per_step": int(state_out / args.steps + 8 + 4),
+                       "what": "upload initial prim+eps (AoS, pinned) + initial_update + K x (cumc_finddt "
+                               "-> dt to host -> clip -> cumc_rungekutta) + download prim/cons/eps/bcell"}
+        sim2.close()
+
+    # ---- CPU baseline: the restatement on the host cores (rank 0, N=1) -------
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        nz = calibrate_slab(n, 6.0)
+        rate, threads, el = cpu_reference_rate(n, nz, 2, 1)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"Orszag-Tang {n}x{n}x{nz} slab at cell size 1/{n}, 2 RK3 steps after 1 "
+                                          f"warm-up ({el:.1f} s; FP64 C++ restatement, OpenMP)"}
+    sim.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,58 @@
+"""Build recipe of the CUDA library (sm_100a) and of the CPU oracle.
+
+``build_library()`` compiles cumpic_b200/csrc/cumc_api.cu with nvcc into
+cumpic_b200/libcumc_b200.so. FMA contraction is off so that the FP64 path is
+bit-compatible with the FP64 restatement used as the test oracle.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libcumc_b200.so")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17", "--fmad=false",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+    "-shared",
+]
+
+
+def _sources():
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh"))] + [
+        os.path.join(ROOT, "include", "cumc.h")]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_library(force: bool = False, verbose: bool = False) -> str:
+    if force or _stale(LIB, _sources()):
+        cmd = ["nvcc", *NVCC_FLAGS, "-o", LIB + ".tmp", os.path.join(CSRC, "cumc_api.cu")]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+def build_oracle(force: bool = False) -> str:
+    """Compile the FP64 CPU oracle (test infrastructure) via oracle/Makefile."""
+    args = ["make", "-s", "-C", os.path.join(ROOT, "oracle")]
+    if force:
+        subprocess.run(args + ["clean"], check=True)
+    subprocess.run(args, check=True)
+    return os.path.join(ROOT, "oracle", "build", "libcumc_oracle.so")
+
+
+if __name__ == "__main__":
+    print(build_library(force=True, verbose=True))
+    print(build_oracle())

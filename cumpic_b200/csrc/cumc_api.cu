@@ -1,0 +1,750 @@
+// cumc_api.cu — C-ABI of the B200 CUMC3D hot path (declared in include/cumc.h).
+//
+// Host side: config validation (solver/setup.f90:121-230), the per-axis
+// tables, device allocation, the RK3 stage sequence of
+// solver/rungekutta.f90:12-148 and the main-loop driver of
+// solver/main.f90:127-143 as a CUDA graph.
+#include "../../include/cumc.h"
+#include "cumc_kernels.cuh"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace cumc;
+
+namespace {
+thread_local std::string g_init_error;
+
+struct ProfEvent {
+    int cls;
+    cudaEvent_t a, b;
+};
+}  // namespace
+
+struct cumc_ctx {
+    cumc_config cfg{};
+    Box box{};
+    int coord = 1, model = 1, recon = 4;
+    double ggas = 5.0 / 3.0, cfl = 0.4;
+    int flag[6]{};
+    signed char fac[6][8]{};
+    std::string err;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+
+    std::vector<void*> allocs;
+    Tabs tabs{};
+    double* w[5]{};
+    double* bc[3]{};
+    double* eps = nullptr;
+    double* U[2][8]{};
+    double* F[3][7]{};
+    double* E[3]{};
+    double* L[8]{};
+    double* staging = nullptr;
+    double** dsoa = nullptr;   // device array of 8 pointers for the transposes
+    double* scal = nullptr;    // dt, t
+    unsigned long long* dtmin = nullptr;
+    int* ints = nullptr;       // steps, done
+    unsigned int* flag_dev = nullptr;
+    double* divb_part = nullptr;
+    double* host_pinned = nullptr;  // 8 doubles of pinned host scratch
+    int cur = 0;
+    bool uploaded = false, ready = false;
+
+    bool prof_on = false;
+    std::vector<ProfEvent> prof;
+    int prof_launches[CUMC_K_COUNT]{};
+    double prof_ms[CUMC_K_COUNT]{};
+    long long launches = 0;
+
+    cudaGraphExec_t graph_exec = nullptr;
+    double graph_t_end = 0.0;
+    long long graph_launches_per_step = 0;
+
+    int fail(int code, const char* fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        err = buf;
+        return code;
+    }
+};
+
+namespace {
+
+int cuda_fail(cumc_ctx* c, cudaError_t e, const char* what) {
+    return c->fail(CUMC_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CUMC_CHECK(expr)                                              \
+    do {                                                              \
+        cudaError_t e_ = (expr);                                      \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, #expr);        \
+    } while (0)
+
+template <typename T>
+int dalloc(cumc_ctx* c, T** p, size_t n) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return c->fail(CUMC_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    }
+    c->allocs.push_back(q);
+    *p = static_cast<T*>(q);
+    return CUMC_OK;
+}
+
+template <typename K, typename... Args>
+void launch(cumc_ctx* c, int cls, long long nthreads, int block, K kern, Args... args) {
+    if (nthreads <= 0) return;
+    const unsigned grid = (unsigned)((nthreads + block - 1) / block);
+    ProfEvent pe{cls, nullptr, nullptr};
+    const bool rec = c->prof_on && cls >= 0;
+    if (rec) {
+        cudaEventCreate(&pe.a);
+        cudaEventCreate(&pe.b);
+        cudaEventRecord(pe.a, c->stream);
+    }
+    kern<<<grid, block, 0, c->stream>>>(args...);
+    ++c->launches;
+    if (rec) {
+        cudaEventRecord(pe.b, c->stream);
+        c->prof.push_back(pe);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// per-axis tables
+// ---------------------------------------------------------------------------
+constexpr int NTAB_AXIS = 11;
+constexpr int NTAB_X = 4, NTAB_Y = 4;
+
+void build_axis(const double* fsrc, int n, std::vector<double>& out, size_t off, int stride) {
+    // out holds NTAB_AXIS arrays of `stride` entries, entry i+3 for index i
+    auto at = [&](int arr, int i) -> double& { return out[off + (size_t)arr * stride + (size_t)(i + 3)]; };
+    auto f = [&](int i) { return fsrc[i + 3]; };
+    for (int i = -3; i <= n + 3; ++i) {
+        at(0, i) = f(i);
+        at(1, i) = i > -3 ? f(i) - f(i - 1) : 0.0;                 // COORD_DX
+        at(2, i) = i > -3 ? 0.5 * (f(i) + f(i - 1)) : 0.0;         // GET_COORD
+    }
+    auto d = [&](int i) { return at(1, i); };
+    for (int i = -1; i <= n + 2; ++i) {  // PPM slope weights (solver/reconstruct.f90:223-247)
+        const double dm1 = d(i - 1), dc = d(i), dp1 = d(i + 1);
+        const double cc1 = dc / ((dm1 + dc) + dp1);
+        const double cc2 = (2.0 * dm1 + dc) / (dp1 + dc);
+        const double cc3 = (dc + 2.0 * dp1) / (dm1 + dc);
+        at(3, i) = cc1 * cc2;
+        at(4, i) = cc1 * cc3;
+    }
+    for (int i = -1; i <= n + 1; ++i) {  // PPM interface weights (solver/reconstruct.f90:211-243)
+        const double dm1 = d(i - 1), dc = d(i), dp1 = d(i + 1), dp2 = d(i + 2);
+        const double a1R = dc / (dc + dp1);
+        const double aR = ((2.0 * dp1) * dc) / (dp1 + dc);
+        const double deltaXR = ((dm1 + dc) + dp1) + dp2;
+        const double z1R = (dm1 + dc) / (2.0 * dc + dp1);
+        const double zR = (dp2 + dp1) / (2.0 * dp1 + dc);
+        at(5, i) = a1R;
+        at(6, i) = (aR * (z1R - zR)) / deltaXR;
+        at(7, i) = ((-dc) * z1R) / deltaXR;
+        at(8, i) = (dp1 * zR) / deltaXR;
+    }
+    for (int i = -1; i <= n + 2; ++i) {  // TVD_MM weights (solver/reconstruct.f90:110-111)
+        at(9, i) = (d(i) + d(i + 1)) / d(i);
+        at(10, i) = (d(i) + d(i - 1)) / d(i);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// stage sequence
+// ---------------------------------------------------------------------------
+template <int DIR>
+void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
+    FaceFlux out;
+    for (int q = 0; q < 7; ++q) out.f[q] = c->F[DIR][q];
+    const long long n = (long long)((DIR == 0 ? b.nx : b.nx + 1) + 1) * ((DIR == 1 ? b.ny : b.ny + 1) + 1) *
+                        ((DIR == 2 ? b.nz : b.nz + 1) + 1);
+    if (c->recon == CUMC_PPMC)
+        launch(c, CUMC_K_SWEEP_X + DIR, n, 128, k_sweep<DIR, 4>, b, c->tabs, pr, c->ggas, out);
+    else
+        launch(c, CUMC_K_SWEEP_X + DIR, n, 128, k_sweep<DIR, 1>, b, c->tabs, pr, c->ggas, out);
+}
+
+template <int COORD, int MODEL>
+void combine_dispatch(cumc_ctx* c, const Box& b, int stage, const Prim& pr, const FaceFlux* ff, const CombineArgs& a) {
+    const long long n = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
+    switch (stage) {
+        case 0: launch(c, CUMC_K_COMBINE, n, 256, k_combine<COORD, MODEL, 0>, b, c->tabs, pr, ff[0], ff[1], ff[2], a); break;
+        case 1: launch(c, CUMC_K_COMBINE, n, 256, k_combine<COORD, MODEL, 1>, b, c->tabs, pr, ff[0], ff[1], ff[2], a); break;
+        case 2: launch(c, CUMC_K_COMBINE, n, 256, k_combine<COORD, MODEL, 2>, b, c->tabs, pr, ff[0], ff[1], ff[2], a); break;
+        default: launch(c, CUMC_K_COMBINE, n, 256, k_combine<COORD, MODEL, 3>, b, c->tabs, pr, ff[0], ff[1], ff[2], a); break;
+    }
+}
+
+template <int COORD>
+void combine_model(cumc_ctx* c, const Box& b, int stage, const Prim& pr, const FaceFlux* ff, const CombineArgs& a) {
+    switch (c->model) {
+        case CUMC_MODEL_NONE: combine_dispatch<COORD, 0>(c, b, stage, pr, ff, a); break;
+        case CUMC_MODEL_RIEMANN: combine_dispatch<COORD, 1>(c, b, stage, pr, ff, a); break;
+        case CUMC_MODEL_TORUS_SPH: combine_dispatch<COORD, 2>(c, b, stage, pr, ff, a); break;
+        default: combine_dispatch<COORD, 3>(c, b, stage, pr, ff, a); break;
+    }
+}
+
+void utop(cumc_ctx* c, const Box& b, double* const* u, bool from_cons) {
+    UtopArgs a;
+    for (int q = 0; q < 8; ++q) a.u[q] = u[q];
+    for (int q = 0; q < 5; ++q) a.w[q] = c->w[q];
+    for (int q = 0; q < 3; ++q) a.bc[q] = c->bc[q];
+    a.eps = c->eps;
+    a.ggas = c->ggas;
+    a.rho_floor = c->cfg.rho_floor;
+    a.eps_floor = c->cfg.eps_floor;
+    a.flag = c->flag_dev;
+    const long long n = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
+#define CUMC_UTOP(M)                                                                         \
+    if (from_cons) launch(c, CUMC_K_UTOP, n, 256, k_utop<M, true>, b, a);                    \
+    else launch(c, CUMC_K_UTOP, n, 256, k_utop<M, false>, b, a);
+    switch (c->model) {
+        case CUMC_MODEL_NONE: CUMC_UTOP(0) break;
+        case CUMC_MODEL_RIEMANN: CUMC_UTOP(1) break;
+        case CUMC_MODEL_TORUS_SPH: CUMC_UTOP(2) break;
+        default: CUMC_UTOP(3) break;
+    }
+#undef CUMC_UTOP
+}
+
+void boundary(cumc_ctx* c, const Box& b, double* const* u) {
+    BoundArgs a;
+    for (int q = 0; q < 5; ++q) a.w[q] = c->w[q];
+    for (int q = 0; q < 3; ++q) a.bc[q] = c->bc[q];
+    a.eps = c->eps;
+    for (int q = 0; q < 3; ++q) a.bf[q] = u[IBX + q];
+    for (int q = 0; q < 6; ++q) a.flag[q] = c->flag[q];
+    a.eps_yout = c->flag[2] == 0 ? 0 : c->flag[3];
+    std::memcpy(a.fac, c->fac, sizeof a.fac);
+    a.ggas = c->ggas;
+    const long long n = 6LL * b.SX * b.SY + 6LL * b.SX * b.nz + 6LL * b.ny * b.nz;
+    switch (c->model) {
+        case CUMC_MODEL_TORUS_SPH: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<2>, b, a); break;
+        case CUMC_MODEL_TORUS_CYN: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<3>, b, a); break;
+        default: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<0>, b, a); break;
+    }
+}
+
+Prim make_prim(cumc_ctx* c, double* const* u) {
+    Prim p;
+    for (int q = 0; q < 5; ++q) p.w[q] = c->w[q];
+    for (int q = 0; q < 3; ++q) p.bc[q] = c->bc[q];
+    for (int q = 0; q < 3; ++q) p.bf[q] = u[IBX + q];
+    return p;
+}
+
+// One SPATIAL + combine + conversions + boundary (solver/rungekutta.f90:38-66).
+// stage 0: SPATIAL only, l_rk stored in c->L.
+void run_stage(cumc_ctx* c, const Box& b, int stage) {
+    double* const* Un = c->U[c->cur];
+    double* const* Ua = c->U[1 - c->cur];
+    double* const* src = (stage <= 1) ? Un : Ua;  // arrays holding prim(ibx:ibz) this stage
+    const Prim pr = make_prim(c, src);
+    sweep<0>(c, b, pr);
+    sweep<1>(c, b, pr);
+    sweep<2>(c, b, pr);
+    FaceFlux ff[3];
+    for (int d = 0; d < 3; ++d)
+        for (int q = 0; q < 7; ++q) ff[d].f[q] = c->F[d][q];
+    EdgeE ee;
+    for (int q = 0; q < 3; ++q) ee.e[q] = c->E[q];
+    launch(c, CUMC_K_EMF, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_emf, b, pr, ff[0], ff[1], ff[2], ee);
+
+    CombineArgs a{};
+    double* const* dst = stage == 1 ? Ua : stage == 2 ? Ua : Un;
+    for (int q = 0; q < 8; ++q) {
+        a.u0[q] = Un[q];
+        a.uc[q] = Ua[q];
+        a.ud[q] = dst[q];
+        a.lrk[q] = c->L[q];
+    }
+    a.dt = c->scal;
+    for (int q = 0; q < 3; ++q) a.ecorn[q] = c->E[q];
+    a.geom_repeat = c->cfg.geom_source_repeat;
+    a.rho_floor = c->cfg.rho_floor;
+    a.r_sh = c->cfg.r_sh;
+    switch (c->coord) {
+        case CUMC_CARTESIAN: combine_model<1>(c, b, stage, pr, ff, a); break;
+        case CUMC_CYLINDRICAL: combine_model<2>(c, b, stage, pr, ff, a); break;
+        default: combine_model<3>(c, b, stage, pr, ff, a); break;
+    }
+    if (stage == 0) return;
+    utop(c, b, dst, true);
+    boundary(c, b, dst);
+}
+
+void rk_step(cumc_ctx* c, const Box& b) {
+    run_stage(c, b, 1);
+    run_stage(c, b, 2);
+    run_stage(c, b, 3);
+}
+
+void finddt_launch(cumc_ctx* c, const Box& b) {
+    launch(c, -1, 1, 1, k_reset_dtmin, c->dtmin);
+    const Prim pr = make_prim(c, c->U[c->cur]);
+    const long long n = (long long)b.nx * b.ny * b.nz;
+    switch (c->coord) {
+        case CUMC_CARTESIAN: launch(c, CUMC_K_FINDDT, n, 256, k_finddt<1>, b, c->tabs, pr, c->ggas, c->cfl, c->dtmin); break;
+        case CUMC_CYLINDRICAL: launch(c, CUMC_K_FINDDT, n, 256, k_finddt<2>, b, c->tabs, pr, c->ggas, c->cfl, c->dtmin); break;
+        default: launch(c, CUMC_K_FINDDT, n, 256, k_finddt<3>, b, c->tabs, pr, c->ggas, c->cfl, c->dtmin); break;
+    }
+}
+
+Clock make_clock(cumc_ctx* c) {
+    Clock k;
+    k.dt = c->scal;
+    k.t = c->scal + 1;
+    k.dtmin = c->dtmin;
+    k.steps = c->ints;
+    k.done = c->ints + 1;
+    return k;
+}
+
+// one main-loop iteration with device-resident dt (solver/main.f90:127-143)
+void loop_step(cumc_ctx* c, double t_end) {
+    Box b = c->box;
+    const Clock k = make_clock(c);
+    launch(c, -1, 1, 1, k_check_done, k, t_end);
+    b.skip = k.done;
+    finddt_launch(c, b);
+    launch(c, -1, 1, 1, k_clip_dt, k, t_end);
+    rk_step(c, b);
+    launch(c, -1, 1, 1, k_advance_time, k);
+}
+
+int check_ready(cumc_ctx* c) {
+    if (!c) return CUMC_ERR_ARG;
+    if (!c->ready) return c->fail(CUMC_ERR_STATE, "cumc_initial_update must run after cumc_upload_state first");
+    return CUMC_OK;
+}
+
+int sync_status(cumc_ctx* c) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    return CUMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cumc_last_error(const cumc_ctx* c) { return c ? c->err.c_str() : g_init_error.c_str(); }
+
+int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
+    g_init_error.clear();
+    if (!cfg || !out) { g_init_error = "null argument"; return CUMC_ERR_ARG; }
+    *out = nullptr;
+    auto bad = [](const char* m) { g_init_error = m; return CUMC_ERR_CONFIG; };
+    if (cfg->nx < 3 || cfg->ny < 3 || cfg->nz < 3) return bad("every direction needs at least 3 active cells (3 ghost layers)");
+    if ((long long)(cfg->nx + 6) * (cfg->ny + 6) * (cfg->nz + 6) >= (1LL << 31))
+        { g_init_error = "grid too large: (nx+6)(ny+6)(nz+6) must stay below 2^31"; return CUMC_ERR_LIMIT; }
+    if (!cfg->xf || !cfg->yf || !cfg->zf) { g_init_error = "face coordinate arrays are required"; return CUMC_ERR_ARG; }
+    if (cfg->coordinate < 1 || cfg->coordinate > 3) return bad("coordinate must be 1 (cartesian), 2 (cylindrical) or 3 (spherical)");
+    if (cfg->recon != CUMC_PPMC && cfg->recon != CUMC_TVDMM) return bad("recon must be CUMC_PPMC or CUMC_TVDMM (the reference implements no other)");
+    if (cfg->solver != CUMC_HLL) return bad("solver must be CUMC_HLL (the reference implements no other)");
+    if (cfg->precision != CUMC_FP64 && cfg->precision != CUMC_MIXED) return bad("precision must be CUMC_FP64 or CUMC_MIXED");
+    if (cfg->precision == CUMC_MIXED) return bad("CUMC_MIXED is not available in this build");
+    if (cfg->model < 0 || cfg->model > 3) return bad("unknown model id");
+    for (int i = 0; i < 6; ++i)
+        if (cfg->boundary_flag[i] < 0 || cfg->boundary_flag[i] > 4) return bad("boundary_flag entries must be 0..4");
+    if (cfg->boundary_flag[0] == 4 || cfg->boundary_flag[1] == 4)
+        return bad("equatorial symmetry is not allowed for the x-boundary (solver/setup.f90:147-151)");
+    if (cfg->boundary_flag[4] == 3 || cfg->boundary_flag[5] == 3)
+        return bad("axial symmetry is not allowed for the z-boundary (solver/setup.f90:206-210)");
+    if (cfg->boundary_flag[2] != 0 && cfg->boundary_flag[3] == 0)
+        return bad("a periodic y-outer face needs a periodic y-inner face (BOUNDARY1D never fills eps there, solver/boundary.f90:211)");
+    if (!(cfg->ggas > 1.0)) return bad("ggas must exceed 1");
+    if (!(cfg->cfl > 0.0)) return bad("cfl must be positive");
+    for (int i = 0; i < 7; ++i)
+        if (cfg->reserved[i] != 0) return bad("reserved fields must be zero");
+
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g_init_error = std::string("no usable CUDA device: ") + cudaGetErrorString(e);
+        return CUMC_ERR_CUDA;
+    }
+
+    auto* c = new cumc_ctx();
+    c->cfg = *cfg;
+    if (c->cfg.geom_source_repeat <= 0) c->cfg.geom_source_repeat = 8;
+    c->coord = cfg->coordinate;
+    c->model = cfg->model;
+    c->recon = cfg->recon;
+    c->ggas = cfg->ggas;
+    c->cfl = cfg->cfl;
+    for (int i = 0; i < 6; ++i) c->flag[i] = cfg->boundary_flag[i];
+    // bfac tables (solver/setup.f90:129-230)
+    for (int s = 0; s < 6; ++s)
+        for (int q = 0; q < 8; ++q) c->fac[s][q] = 1;
+    for (int s = 0; s < 2; ++s) {
+        const int f = c->flag[s];
+        if (f == 2 || f == 3) { c->fac[s][IVX] = -1; c->fac[s][IBX] = -1; }
+        if (f == 3) { c->fac[s][IVZ] = -1; c->fac[s][IBZ] = -1; }
+    }
+    for (int s = 2; s < 4; ++s) {
+        const int f = c->flag[s];
+        if (f == 2 || f == 3) { c->fac[s][IVY] = -1; c->fac[s][IBY] = -1; }
+        if (f == 3) { c->fac[s][IVZ] = -1; c->fac[s][IBZ] = -1; }
+        if (f == 4) { c->fac[s][IVY] = -1; c->fac[s][IBX] = -1; c->fac[s][IBZ] = -1; }
+    }
+    for (int s = 4; s < 6; ++s) {
+        const int f = c->flag[s];
+        if (f == 2) { c->fac[s][IVZ] = -1; c->fac[s][IBZ] = -1; }
+        if (f == 4) { c->fac[s][IVZ] = -1; c->fac[s][IBX] = -1; c->fac[s][IBY] = -1; }
+    }
+
+    Box& b = c->box;
+    b.nx = cfg->nx; b.ny = cfg->ny; b.nz = cfg->nz;
+    b.SX = b.nx + 6; b.SY = b.ny + 6; b.SZ = b.nz + 6;
+    b.skip = nullptr;
+    const size_t NT = (size_t)b.count();
+
+    auto fail_init = [&](int code) {
+        g_init_error = c->err;
+        cumc_free(c);
+        return code;
+    };
+    if ((e = cudaGetDevice(&c->device)) != cudaSuccess) { cuda_fail(c, e, "cudaGetDevice"); return fail_init(CUMC_ERR_CUDA); }
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        cuda_fail(c, e, "cudaStreamCreate");
+        return fail_init(CUMC_ERR_CUDA);
+    }
+
+    // tables
+    const int st[3] = {b.nx + 7, b.ny + 7, b.nz + 7};
+    size_t ntab = 0;
+    size_t off[3];
+    for (int a = 0; a < 3; ++a) { off[a] = ntab; ntab += (size_t)NTAB_AXIS * st[a]; }
+    const size_t offx = ntab; ntab += (size_t)NTAB_X * st[0];
+    const size_t offy = ntab; ntab += (size_t)NTAB_Y * st[1];
+    std::vector<double> h(ntab, 0.0);
+    const double* fsrc[3] = {cfg->xf, cfg->yf, cfg->zf};
+    const int nn[3] = {b.nx, b.ny, b.nz};
+    for (int a = 0; a < 3; ++a) build_axis(fsrc[a], nn[a], h, off[a], st[a]);
+    for (int j = -2; j <= b.nx + 3; ++j) {
+        const double xp = cfg->xf[j + 3], xm = cfg->xf[j + 2];
+        h[offx + 0 * st[0] + j + 3] = xp * xp;
+        h[offx + 1 * st[0] + j + 3] = ((xp * xp) * xp - (xm * xm) * xm) / 3.0;
+        h[offx + 2 * st[0] + j + 3] = ((2.0 * ((xp * xp) * xp - (xm * xm) * xm)) / 3.0) / (xp * xp - xm * xm);
+        h[offx + 3 * st[0] + j + 3] = 0.5 * (xp * xp - xm * xm);
+    }
+    h[offx + 0 * st[0] + 0] = cfg->xf[0] * cfg->xf[0];
+    for (int k = -2; k <= b.ny + 3; ++k) {
+        const double yp = cfg->yf[k + 3], ym = cfg->yf[k + 2];
+        const double yc = 0.5 * (yp + ym);
+        h[offy + 0 * st[1] + k + 3] = std::sin(yp);
+        h[offy + 1 * st[1] + k + 3] = std::cos(ym) - std::cos(yp);
+        h[offy + 2 * st[1] + k + 3] = std::tan(yc);
+        h[offy + 3 * st[1] + k + 3] = std::sin(yc);
+    }
+    h[offy + 0 * st[1] + 0] = std::sin(cfg->yf[0]);
+    double* dtab = nullptr;
+    int rc;
+    if ((rc = dalloc(c, &dtab, ntab)) != CUMC_OK) return fail_init(rc);
+    if ((e = cudaMemcpy(dtab, h.data(), ntab * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess) {
+        cuda_fail(c, e, "table upload");
+        return fail_init(CUMC_ERR_CUDA);
+    }
+    for (int a = 0; a < 3; ++a) {
+        const double* base = dtab + off[a] + 3;
+        AxisTabs& A = c->tabs.ax[a];
+        const double** p[NTAB_AXIS] = {&A.f, &A.d, &A.c, &A.s0, &A.s1, &A.a0, &A.a1, &A.a2, &A.a3, &A.tcf, &A.tcb};
+        for (int q = 0; q < NTAB_AXIS; ++q) *p[q] = base + (size_t)q * st[a];
+    }
+    c->tabs.r2 = dtab + offx + 3;
+    c->tabs.r3d3 = dtab + offx + st[0] + 3;
+    c->tabs.rfac = dtab + offx + 2 * st[0] + 3;
+    c->tabs.hr2 = dtab + offx + 3 * st[0] + 3;
+    c->tabs.sinf = dtab + offy + 3;
+    c->tabs.dcos = dtab + offy + st[1] + 3;
+    c->tabs.tanc = dtab + offy + 2 * st[1] + 3;
+    c->tabs.sinc = dtab + offy + 3 * st[1] + 3;
+
+    // state
+    auto field = [&](double** p) -> int {
+        int r = dalloc(c, p, NT);
+        if (r != CUMC_OK) return r;
+        return cudaMemset(*p, 0, NT * sizeof(double)) == cudaSuccess ? CUMC_OK : CUMC_ERR_CUDA;
+    };
+    for (int q = 0; q < 5; ++q) if ((rc = field(&c->w[q])) != CUMC_OK) return fail_init(rc);
+    for (int q = 0; q < 3; ++q) if ((rc = field(&c->bc[q])) != CUMC_OK) return fail_init(rc);
+    if ((rc = field(&c->eps)) != CUMC_OK) return fail_init(rc);
+    for (int s = 0; s < 2; ++s)
+        for (int q = 0; q < 8; ++q) if ((rc = field(&c->U[s][q])) != CUMC_OK) return fail_init(rc);
+    for (int d = 0; d < 3; ++d)
+        for (int q = 0; q < 7; ++q) if ((rc = field(&c->F[d][q])) != CUMC_OK) return fail_init(rc);
+    for (int q = 0; q < 3; ++q) if ((rc = field(&c->E[q])) != CUMC_OK) return fail_init(rc);
+    if ((rc = dalloc(c, &c->dsoa, 8)) != CUMC_OK) return fail_init(rc);
+    if ((rc = dalloc(c, &c->scal, 4)) != CUMC_OK) return fail_init(rc);
+    if ((rc = dalloc(c, &c->dtmin, 1)) != CUMC_OK) return fail_init(rc);
+    if ((rc = dalloc(c, &c->ints, 4)) != CUMC_OK) return fail_init(rc);
+    if ((rc = dalloc(c, &c->flag_dev, 1)) != CUMC_OK) return fail_init(rc);
+    cudaMemset(c->scal, 0, 4 * sizeof(double));
+    cudaMemset(c->ints, 0, 4 * sizeof(int));
+    cudaMemset(c->flag_dev, 0, sizeof(unsigned));
+    if ((e = cudaMallocHost(&c->host_pinned, 8 * sizeof(double))) != cudaSuccess) {
+        cuda_fail(c, e, "cudaMallocHost");
+        return fail_init(CUMC_ERR_NOMEM);
+    }
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) { cuda_fail(c, e, "init"); return fail_init(CUMC_ERR_CUDA); }
+    *out = c;
+    return CUMC_OK;
+}
+
+int cumc_free(cumc_ctx* c) {
+    if (!c) return CUMC_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& pe : c->prof) { cudaEventDestroy(pe.a); cudaEventDestroy(pe.b); }
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    for (void* p : c->allocs) cudaFree(p);
+    if (c->host_pinned) cudaFreeHost(c->host_pinned);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return CUMC_OK;
+}
+
+// staging buffer for the AoS <-> SoA transposes, allocated on first use
+static int ensure_staging(cumc_ctx* c) {
+    if (c->staging) return CUMC_OK;
+    return dalloc(c, &c->staging, 8 * (size_t)c->box.count());
+}
+
+static int put_soa(cumc_ctx* c, const double* host, int nv, double* const* dst) {
+    const size_t NT = (size_t)c->box.count();
+    int rc = ensure_staging(c);
+    if (rc != CUMC_OK) return rc;
+    CUMC_CHECK(cudaMemcpyAsync(c->dsoa, dst, nv * sizeof(double*), cudaMemcpyHostToDevice, c->stream));
+    CUMC_CHECK(cudaMemcpyAsync(c->staging, host, nv * NT * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    launch(c, -1, (long long)NT, 256, k_aos_to_soa, (long long)NT, nv, (const double*)c->staging, c->dsoa);
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    return sync_status(c);
+}
+
+static int get_soa(cumc_ctx* c, double* host, int nv, const double* const* srcp) {
+    const size_t NT = (size_t)c->box.count();
+    int rc = ensure_staging(c);
+    if (rc != CUMC_OK) return rc;
+    CUMC_CHECK(cudaMemcpyAsync(c->dsoa, srcp, nv * sizeof(double*), cudaMemcpyHostToDevice, c->stream));
+    launch(c, -1, (long long)NT, 256, k_soa_to_aos, (long long)NT, nv, c->staging, (const double* const*)c->dsoa);
+    CUMC_CHECK(cudaMemcpyAsync(host, c->staging, nv * NT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    return sync_status(c);
+}
+
+int cumc_upload_state(cumc_ctx* c, const double* prim, const double* eps) {
+    if (!c || !prim || !eps) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
+    double* dst[8] = {c->w[0], c->w[1], c->w[2], c->w[3], c->w[4], c->U[c->cur][IBX], c->U[c->cur][IBY], c->U[c->cur][IBZ]};
+    int rc = put_soa(c, prim, 8, dst);
+    if (rc != CUMC_OK) return rc;
+    double* de[1] = {c->eps};
+    rc = put_soa(c, eps, 1, de);
+    if (rc != CUMC_OK) return rc;
+    c->uploaded = true;
+    c->ready = false;
+    return CUMC_OK;
+}
+
+int cumc_download_state(cumc_ctx* c, double* prim, double* cons, double* eps, double* bcell) {
+    if (!c) return CUMC_ERR_ARG;
+    int rc;
+    double* const* u = c->U[c->cur];
+    if (prim) {
+        const double* s[8] = {c->w[0], c->w[1], c->w[2], c->w[3], c->w[4], u[IBX], u[IBY], u[IBZ]};
+        if ((rc = get_soa(c, prim, 8, s)) != CUMC_OK) return rc;
+    }
+    if (cons) {
+        const double* s[8] = {u[0], u[1], u[2], u[3], u[4], u[5], u[6], u[7]};
+        if ((rc = get_soa(c, cons, 8, s)) != CUMC_OK) return rc;
+    }
+    if (eps) {
+        const double* s[1] = {c->eps};
+        if ((rc = get_soa(c, eps, 1, s)) != CUMC_OK) return rc;
+    }
+    if (bcell) {
+        const double* s[3] = {c->bc[0], c->bc[1], c->bc[2]};
+        if ((rc = get_soa(c, bcell, 3, s)) != CUMC_OK) return rc;
+    }
+    return CUMC_OK;
+}
+
+int cumc_initial_update(cumc_ctx* c) {
+    if (!c) return CUMC_ERR_ARG;
+    if (!c->uploaded) return c->fail(CUMC_ERR_STATE, "cumc_upload_state must come first");
+    utop(c, c->box, c->U[c->cur], false);
+    boundary(c, c->box, c->U[c->cur]);
+    c->ready = true;
+    return sync_status(c);
+}
+
+int cumc_finddt(cumc_ctx* c, double* dt) {
+    int rc = check_ready(c);
+    if (rc != CUMC_OK) return rc;
+    if (!dt) return c->fail(CUMC_ERR_ARG, "null dt");
+    finddt_launch(c, c->box);
+    CUMC_CHECK(cudaMemcpyAsync(c->host_pinned, c->dtmin, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    CUMC_CHECK(cudaMemcpyAsync(c->host_pinned + 1, c->flag_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    if ((rc = sync_status(c)) != CUMC_OK) return rc;
+    std::memcpy(dt, c->host_pinned, sizeof(double));
+    unsigned fl;
+    std::memcpy(&fl, c->host_pinned + 1, sizeof(unsigned));
+    if (fl & 1u) return c->fail(CUMC_ERR_NONFINITE, "non-finite density, velocity or pressure in the evolved state");
+    return CUMC_OK;
+}
+
+int cumc_rungekutta(cumc_ctx* c, double dt) {
+    int rc = check_ready(c);
+    if (rc != CUMC_OK) return rc;
+    launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
+    rk_step(c, c->box);
+    return sync_status(c);
+}
+
+int cumc_spatial(cumc_ctx* c) {
+    int rc = check_ready(c);
+    if (rc != CUMC_OK) return rc;
+    const size_t NT = (size_t)c->box.count();
+    if (!c->L[0])
+        for (int q = 0; q < 8; ++q) {
+            if ((rc = dalloc(c, &c->L[q], NT)) != CUMC_OK) return rc;
+            CUMC_CHECK(cudaMemsetAsync(c->L[q], 0, NT * sizeof(double), c->stream));
+        }
+    run_stage(c, c->box, 0);
+    return sync_status(c);
+}
+
+int cumc_download_lrk(cumc_ctx* c, double* lrk) {
+    if (!c || !lrk) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
+    if (!c->L[0]) return c->fail(CUMC_ERR_STATE, "cumc_spatial has not run");
+    const double* s[8] = {c->L[0], c->L[1], c->L[2], c->L[3], c->L[4], c->L[5], c->L[6], c->L[7]};
+    return get_soa(c, lrk, 8, s);
+}
+
+int cumc_divb(cumc_ctx* c, double* maxdb_signed, double* maxabs_norm) {
+    int rc = check_ready(c);
+    if (rc != CUMC_OK) return rc;
+    const Box& b = c->box;
+    const long long n = (long long)b.nx * b.ny * b.nz;
+    const int nblk = (int)((n + 255) / 256);
+    if (!c->divb_part && (rc = dalloc(c, &c->divb_part, 3 * (size_t)nblk)) != CUMC_OK) return rc;
+    double* const* u = c->U[c->cur];
+    switch (c->coord) {
+        case CUMC_CARTESIAN: launch(c, -1, n, 256, k_divb<1>, b, c->tabs, (const double*)u[IBX], (const double*)u[IBY], (const double*)u[IBZ], c->divb_part); break;
+        case CUMC_CYLINDRICAL: launch(c, -1, n, 256, k_divb<2>, b, c->tabs, (const double*)u[IBX], (const double*)u[IBY], (const double*)u[IBZ], c->divb_part); break;
+        default: launch(c, -1, n, 256, k_divb<3>, b, c->tabs, (const double*)u[IBX], (const double*)u[IBY], (const double*)u[IBZ], c->divb_part); break;
+    }
+    std::vector<double> h(3 * (size_t)nblk);
+    CUMC_CHECK(cudaMemcpyAsync(h.data(), c->divb_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    double smax = 0.0, amax = 0.0, fmx = 0.0;  // the reference starts maxdb at 0 (solver/mhd.f90:41)
+    for (int i = 0; i < nblk; ++i) {
+        smax = std::fmax(smax, h[3 * i]);
+        amax = std::fmax(amax, h[3 * i + 1]);
+        fmx = std::fmax(fmx, h[3 * i + 2]);
+    }
+    if (maxdb_signed) *maxdb_signed = smax;
+    if (maxabs_norm) *maxabs_norm = fmx > 0.0 ? amax / fmx : 0.0;
+    return sync_status(c);
+}
+
+int cumc_advance(cumc_ctx* c, int nsteps, double t_end, double* t_inout, int* steps_done) {
+    int rc = check_ready(c);
+    if (rc != CUMC_OK) return rc;
+    if (nsteps < 0 || !t_inout) return c->fail(CUMC_ERR_ARG, "nsteps must be >= 0 and t_inout non-null");
+    launch(c, -1, 1, 1, k_set_scalar, c->scal + 1, *t_inout);
+    CUMC_CHECK(cudaMemsetAsync(c->ints, 0, 2 * sizeof(int), c->stream));
+    if (c->prof_on) {
+        for (int s = 0; s < nsteps; ++s) loop_step(c, t_end);
+    } else if (nsteps > 0) {
+        if (!c->graph_exec || c->graph_t_end != t_end) {
+            if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+            cudaGraph_t g;
+            CUMC_CHECK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            const long long before = c->launches;
+            loop_step(c, t_end);
+            const long long per_step = c->launches - before;
+            c->launches = before;
+            CUMC_CHECK(cudaStreamEndCapture(c->stream, &g));
+            cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+            c->graph_t_end = t_end;
+            c->graph_launches_per_step = per_step;
+        }
+        for (int s = 0; s < nsteps; ++s) {
+            CUMC_CHECK(cudaGraphLaunch(c->graph_exec, c->stream));
+            c->launches += c->graph_launches_per_step;
+        }
+    }
+    CUMC_CHECK(cudaMemcpyAsync(c->host_pinned, c->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUMC_CHECK(cudaMemcpyAsync(c->host_pinned + 1, c->ints, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUMC_CHECK(cudaMemcpyAsync(c->host_pinned + 2, c->flag_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    if ((rc = sync_status(c)) != CUMC_OK) return rc;
+    std::memcpy(t_inout, c->host_pinned, sizeof(double));
+    int st;
+    std::memcpy(&st, c->host_pinned + 1, sizeof(int));
+    if (steps_done) *steps_done = st;
+    unsigned fl;
+    std::memcpy(&fl, c->host_pinned + 2, sizeof(unsigned));
+    if (fl & 1u) return c->fail(CUMC_ERR_NONFINITE, "non-finite density, velocity or pressure in the evolved state");
+    return CUMC_OK;
+}
+
+int cumc_get_stream(cumc_ctx* c, void** stream) {
+    if (!c || !stream) return CUMC_ERR_ARG;
+    *stream = (void*)c->stream;
+    return CUMC_OK;
+}
+
+int cumc_profile(cumc_ctx* c, int enable) {
+    if (!c) return CUMC_ERR_ARG;
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    for (auto& pe : c->prof) { cudaEventDestroy(pe.a); cudaEventDestroy(pe.b); }
+    c->prof.clear();
+    for (int i = 0; i < CUMC_K_COUNT; ++i) { c->prof_launches[i] = 0; c->prof_ms[i] = 0.0; }
+    c->prof_on = enable != 0;
+    return CUMC_OK;
+}
+
+int cumc_profile_read(cumc_ctx* c, int which, int* launches, double* ms) {
+    if (!c || which < 0 || which >= CUMC_K_COUNT) return CUMC_ERR_ARG;
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    for (auto& pe : c->prof) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, pe.a, pe.b);
+        c->prof_launches[pe.cls] += 1;
+        c->prof_ms[pe.cls] += t;
+        cudaEventDestroy(pe.a);
+        cudaEventDestroy(pe.b);
+    }
+    c->prof.clear();
+    if (launches) *launches = c->prof_launches[which];
+    if (ms) *ms = c->prof_ms[which];
+    return CUMC_OK;
+}
+
+int cumc_launch_count(cumc_ctx* c, long long* count) {
+    if (!c || !count) return CUMC_ERR_ARG;
+    *count = c->launches;
+    return CUMC_OK;
+}
+
+}  // extern "C"

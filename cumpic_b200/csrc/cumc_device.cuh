@@ -1,0 +1,267 @@
+// cumc_device.cuh — device-side data layout and per-cell arithmetic of the
+// CUMC3D hot path on B200 (sm_100a).
+//
+// Layout in HBM: structure of arrays. Every field is one FP64 array over the
+// ghosted box (-2:n+3)^3 with x fastest, so a warp reads 32 consecutive x
+// cells (256 B) per variable. The reference keeps the 8 equations
+// interleaved per cell (AoS, solver/setup.f90:257); the library transposes
+// once at upload/download.
+//
+// Every arithmetic expression below keeps the operation order of the
+// reference subroutine it cites; the parity build uses --fmad=false so that
+// no multiply-add is contracted and the FP64 path reproduces the FP64 CPU
+// restatement bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cumc {
+
+constexpr int NG = 3;  // ghost layers (solver/definition.f90:54)
+
+// Box geometry: strides of the ghosted SoA arrays.
+struct Box {
+    int nx, ny, nz;
+    int SX, SY, SZ;  // nx+6, ny+6, nz+6
+    const int* skip;  // device flag: when non-null and set, kernels return at once
+                      // (the time loop has reached t_end inside a captured graph)
+    __host__ __device__ __forceinline__ int idx(int j, int k, int l) const {
+        return (j + 2) + SX * ((k + 2) + SY * (l + 2));
+    }
+    __host__ __device__ __forceinline__ long long count() const { return (long long)SX * SY * SZ; }
+};
+
+// Per-axis 1-D tables (pointers pre-offset so that t[i] is valid for
+// i in -3..n+3). All values are computed on the host with the formulas of the
+// reference so that the device reads the same doubles the reference would
+// recompute inline.
+struct AxisTabs {
+    const double* f;    // face coordinate xF(i)                   (solver/coords.f90:24-32)
+    const double* d;    // cell width  xF(i)-xF(i-1)               (COORD_DX, :91-93)
+    const double* c;    // cell centre 0.5*(xF(i)+xF(i-1))         (GET_COORD, :63-65)
+    const double* s0;   // PPM slope weight b0c of cell i          (solver/reconstruct.f90:246)
+    const double* s1;   // PPM slope weight b1c of cell i          (:247)
+    const double* a0;   // PPM interface weights a0p..a3p of the   (:240-243)
+    const double* a1;   //   face between cell i and i+1; equal to
+    const double* a2;   //   a0m..a3m of cell i+1
+    const double* a3;
+    const double* tcf;  // TVD_MM cf of cell i                     (:110)
+    const double* tcb;  // TVD_MM cb of cell i                     (:111)
+};
+
+struct Tabs {
+    AxisTabs ax[3];
+    // x-axis metric factors (solver/coords.f90:173-415)
+    const double* r2;     // xF(j)*xF(j)
+    const double* r3d3;   // (xF(j)^3 - xF(j-1)^3)/3
+    const double* rfac;   // (2*(xF(j)^3-xF(j-1)^3)/3)/(xF(j)^2-xF(j-1)^2)
+    const double* hr2;    // 0.5*(xF(j)^2 - xF(j-1)^2)
+    // y-axis metric factors
+    const double* sinf;   // sin(yF(k))
+    const double* dcos;   // cos(yF(k-1)) - cos(yF(k))
+    const double* tanc;   // tan(y-centre of cell k)
+    const double* sinc;   // sin(y-centre of cell k)
+};
+
+// Equation identifiers (solver/setup.f90:49-116), zero-based here.
+enum { IRHO = 0, IVX = 1, IVY = 2, IVZ = 3, ITAU = 4, IBX = 5, IBY = 6, IBZ = 7 };
+
+// ---------------------------------------------------------------------------
+// reconstruction
+// ---------------------------------------------------------------------------
+
+// van Leer-limited PPM slope of a cell from its neighbours
+// (solver/reconstruct.f90:254-280). The reference evaluates this three times
+// per call (dmm1, dmc, dmp1); the three forms are the same expression of the
+// cell's own (vm, vc, vp) and weights, so it is computed once per cell.
+template <typename R>
+__device__ __forceinline__ R ppm_slope(R vm, R vc, R vp, R b0, R b1) {
+    const R delta = b0 * (vp - vc) + b1 * (vc - vm);
+    if ((vp - vc) * (vc - vm) > R(0))
+        return fmin(fmin(fabs(delta), R(2) * fabs(vc - vm)), R(2) * fabs(vc - vp)) * copysign(R(1), delta);
+    return R(0);
+}
+
+// Unlimited PPM value at the face between cell c and c+1
+// (solver/reconstruct.f90:285; identical to :286 evaluated by cell c+1).
+template <typename R>
+__device__ __forceinline__ R ppm_face(R vc, R vp, R dmc, R dmp, R a0, R a1, R a2, R a3) {
+    return (((vc + a0 * (vp - vc)) + a1 * (vp - vc)) + a2 * dmp) + a3 * dmc;
+}
+
+// Extremum and overshoot fixes of one cell (solver/reconstruct.f90:289-307).
+// The second test reads the already-modified left value, as the reference does.
+template <typename R>
+__device__ __forceinline__ void ppm_fix(R vc, R vl, R vr, R& vm_out, R& vp_out) {
+    vm_out = vl;
+    vp_out = vr;
+    if ((vr - vc) * (vc - vl) <= R(0)) {
+        vp_out = vc;
+        vm_out = vc;
+    } else {
+        if ((vr - vl) * ((vl - R(3) * vc) + R(2) * vr) < R(0)) vm_out = R(3) * vc - R(2) * vr;
+        if ((vp_out - vm_out) * ((R(3) * vc - R(2) * vl) - vr) < R(0)) vp_out = R(3) * vc - R(2) * vl;
+    }
+}
+
+// TVD minmod slope of a cell (solver/reconstruct.f90:110-118).
+template <typename R>
+__device__ __forceinline__ R tvd_slope(R vm, R vc, R vp, R cf, R cb) {
+    const R dqf = (R(2) * (vp - vc)) / cf;
+    const R dqb = (R(2) * (vc - vm)) / cb;
+    return (R(0.5) * (copysign(R(1), dqf) + copysign(R(1), dqb))) * fmin(fabs(dqf), fabs(dqb));
+}
+
+// ---------------------------------------------------------------------------
+// HLL Riemann solver at one face (solver/rsolver.f90:43-130)
+// ---------------------------------------------------------------------------
+
+// compute_signalspeed (solver/definition.f90:394-410)
+template <typename R>
+__device__ __forceinline__ R signalspeed(R cs, R bn, R bt1, R bt2, R rho) {
+    const R a2 = cs * cs;
+    const R a4 = a2 * a2;
+    const R b2n = (bn * bn) / rho;
+    const R b2t1 = (bt1 * bt1) / rho;
+    const R b2t2 = (bt2 * bt2) / rho;
+    const R b2 = (b2n + b2t1) + b2t2;
+    const R b4 = b2 * b2;
+    return sqrt(R(0.5) * ((a2 + b2) + sqrt(fmax(((a4 + b4) + (R(2) * b2) * a2) - (R(4) * a2) * b2n, R(0)))));
+}
+
+// compute_roe (solver/definition.f90:387-392)
+template <typename R>
+__device__ __forceinline__ R roe_avg(R xl, R xr, R sl, R sr) {
+    // sl, sr = sqrt(rhoL), sqrt(rhoR): the reference takes each DSQRT again
+    // per call; the value is the same.
+    return (sl * xl + sr * xr) / (sl + sr);
+}
+
+// compute_fluxhll (solver/definition.f90:380-385)
+template <typename R>
+__device__ __forceinline__ R fluxhll(R yl, R yr, R xl, R xr, R sl, R sr) {
+    return ((sr * yl - sl * yr) + (sl * sr) * (xr - xl)) / (sr - sl);
+}
+
+// One side of the face: conserved state (PtoU_MHD_face, solver/ptou_face.f90:34-88)
+// and physical flux (Ptof_MHD, solver/flux.f90:163-262). w is in natural
+// order (rho, vx, vy, vz, p, bx, by, bz); u and f receive the 8 components.
+template <int DIR, typename R>
+__device__ __forceinline__ void side_state(const R w[8], R ggas, R u[8], R f[8]) {
+    constexpr int ivn = IVX + DIR, ivt1 = IVX + (DIR + 1) % 3, ivt2 = IVX + (DIR + 2) % 3;
+    constexpr int ibn = IBX + DIR, ibt1 = IBX + (DIR + 1) % 3, ibt2 = IBX + (DIR + 2) % 3;
+    const R rho = w[IRHO], vx = w[IVX], vy = w[IVY], vz = w[IVZ], p = w[ITAU];
+    const R bx = w[IBX], by = w[IBY], bz = w[IBZ];
+    const R e = (p / rho) / (ggas - R(1));  // EOS_EPSILON (model/riemann/src/eos.f90:194)
+    const R vsquare = (vx * vx + vy * vy) + vz * vz;
+    const R bsquare = (bx * bx + by * by) + bz * bz;
+    u[IRHO] = rho;
+    u[IVX] = vx * rho;
+    u[IVY] = vy * rho;
+    u[IVZ] = vz * rho;
+    u[ITAU] = rho * (e + R(0.5) * vsquare) + R(0.5) * bsquare;
+    u[IBX] = bx;
+    u[IBY] = by;
+    u[IBZ] = bz;
+    const R vdotb = (bx * vx + by * vy) + bz * vz;
+    const R vn = w[ivn], bn = w[ibn];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) f[i] = u[i] * vn;
+    f[ivn] = ((f[ivn] + p) + R(0.5) * bsquare) - bn * bn;
+    f[ivt1] = f[ivt1] - bn * w[ibt1];
+    f[ivt2] = f[ivt2] - bn * w[ibt2];
+    f[ITAU] = (f[ITAU] + (p + R(0.5) * bsquare) * vn) - bn * vdotb;
+    f[ibn] = R(0);
+    f[ibt1] = vn * w[ibt1] - w[ivt1] * bn;
+    f[ibt2] = vn * w[ibt2] - w[ivt2] * bn;
+}
+
+// HLL flux at a face from the left and right primitive states.
+template <int DIR, typename R>
+__device__ __forceinline__ void hll_flux(const R wl[8], const R wr[8], R ggas, R flux[8]) {
+    constexpr int ivn = IVX + DIR;
+    constexpr int ibn = IBX + DIR, ibt1 = IBX + (DIR + 1) % 3, ibt2 = IBX + (DIR + 2) % 3;
+    R ul[8], ur[8], fl[8], fr[8];
+    side_state<DIR>(wl, ggas, ul, fl);
+    side_state<DIR>(wr, ggas, ur, fr);
+    // EOS_SOUNDSPEED (model/riemann/src/eos.f90:168)
+    const R csL = sqrt((ggas * wl[ITAU]) / wl[IRHO]);
+    const R csR = sqrt((ggas * wr[ITAU]) / wr[IRHO]);
+    const R cfsL = signalspeed(csL, wl[ibn], wl[ibt1], wl[ibt2], wl[IRHO]);
+    const R cfsR = signalspeed(csR, wr[ibn], wr[ibt1], wr[ibt2], wr[IRHO]);
+    const R sqL = sqrt(wl[IRHO]), sqR = sqrt(wr[IRHO]);
+    const R ubar = roe_avg(wl[ivn], wr[ivn], sqL, sqR);
+    const R cbar = roe_avg(cfsL, cfsR, sqL, sqR);
+    const R sL = fmin(wl[ivn] - cfsL, ubar - cbar);
+    const R sR = fmax(wr[ivn] + cfsR, ubar + cbar);
+    if (sL >= R(0)) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) flux[i] = fl[i];
+    } else if (sL <= R(0) && sR >= R(0)) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) flux[i] = fluxhll(fl[i], fr[i], ul[i], ur[i], sL, sR);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) flux[i] = fr[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// geometry (solver/coords.f90) from the 1-D tables
+// ---------------------------------------------------------------------------
+
+// GEOM_FLUX (solver/coords.f90:231-302) for direction DIR at cell (j,k,l)
+template <int COORD, int DIR>
+__device__ __forceinline__ void geom_flux(const Tabs& T, int j, int k, int l, double& gp, double& gc, double& gm) {
+    if (COORD == 1) {
+        gp = 1.0;
+        gm = 1.0;
+        gc = DIR == 0 ? T.ax[0].d[j] : DIR == 1 ? T.ax[1].d[k] : T.ax[2].d[l];
+    } else if (COORD == 2) {
+        if (DIR == 0) { gp = T.ax[0].f[j]; gm = T.ax[0].f[j - 1]; gc = T.ax[0].c[j] * T.ax[0].d[j]; }
+        else if (DIR == 1) { gp = 1.0; gm = 1.0; gc = T.ax[0].c[j] * T.ax[1].d[k]; }
+        else { gp = 1.0; gm = 1.0; gc = T.ax[2].d[l]; }
+    } else {
+        if (DIR == 0) { gp = T.r2[j]; gm = T.r2[j - 1]; gc = T.r3d3[j]; }
+        else if (DIR == 1) { gp = T.sinf[k]; gm = T.sinf[k - 1]; gc = T.rfac[j] * T.dcos[k]; }
+        else { gp = 1.0; gm = 1.0; gc = ((T.rfac[j] * T.dcos[k]) * T.ax[2].d[l]) / T.ax[1].d[k]; }
+    }
+}
+
+// GEOM_CT (solver/coords.f90:310-415)
+struct CTf {
+    double bx_ez_m, bx_ez_c, bx_ez_p, bx_ey_m, bx_ey_c, bx_ey_p;
+    double by_ex_m, by_ex_c, by_ex_p, by_ez_m, by_ez_c, by_ez_p;
+    double bz_ex_m, bz_ex_c, bz_ex_p, bz_ey_m, bz_ey_c, bz_ey_p;
+};
+template <int COORD>
+__device__ __forceinline__ void geom_ct(const Tabs& T, int j, int k, int l, CTf& g) {
+    const double dxl = T.ax[0].d[j], dyl = T.ax[1].d[k], dzl = T.ax[2].d[l];
+    if (COORD == 1) {
+        g.bx_ez_m = 1.0; g.bx_ez_c = dyl; g.bx_ez_p = 1.0;
+        g.bx_ey_m = 1.0; g.bx_ey_c = dzl; g.bx_ey_p = 1.0;
+        g.by_ex_m = 1.0; g.by_ex_c = dzl; g.by_ex_p = 1.0;
+        g.by_ez_m = 1.0; g.by_ez_c = dxl; g.by_ez_p = 1.0;
+        g.bz_ey_m = 1.0; g.bz_ey_c = dxl; g.bz_ey_p = 1.0;
+        g.bz_ex_m = 1.0; g.bz_ex_c = dyl; g.bz_ex_p = 1.0;
+    } else if (COORD == 2) {
+        const double x = T.ax[0].c[j];
+        g.bx_ez_m = 1.0; g.bx_ez_c = dyl * T.ax[0].f[j]; g.bx_ez_p = 1.0;
+        g.bx_ey_m = 1.0; g.bx_ey_c = dzl; g.bx_ey_p = 1.0;
+        g.by_ex_m = 1.0; g.by_ex_c = dzl; g.by_ex_p = 1.0;
+        g.by_ez_m = 1.0; g.by_ez_c = dxl; g.by_ez_p = 1.0;
+        g.bz_ey_m = T.ax[0].f[j - 1]; g.bz_ey_c = x * dxl; g.bz_ey_p = T.ax[0].f[j];
+        g.bz_ex_m = 1.0; g.bz_ex_c = x * dyl; g.bz_ex_p = 1.0;
+    } else {
+        const double x = T.ax[0].c[j];
+        const double dc = T.dcos[k];
+        g.bx_ez_m = T.sinf[k - 1]; g.bx_ez_c = T.ax[0].f[j] * dc; g.bx_ez_p = T.sinf[k];
+        g.bx_ey_m = 1.0; g.bx_ey_c = ((T.ax[0].f[j] * dc) * dzl) / dyl; g.bx_ey_p = 1.0;
+        g.by_ex_m = 1.0; g.by_ex_c = (x * T.sinf[k]) * dzl; g.by_ex_p = 1.0;
+        g.by_ez_m = T.ax[0].f[j - 1]; g.by_ez_c = x * dxl; g.by_ez_p = T.ax[0].f[j];
+        g.bz_ey_m = T.ax[0].f[j - 1]; g.bz_ey_c = x * dxl; g.bz_ey_p = T.ax[0].f[j];
+        g.bz_ex_m = 1.0; g.bz_ex_c = x * dyl; g.bz_ex_p = 1.0;
+    }
+}
+
+}  // namespace cumc

@@ -1,0 +1,657 @@
+// cumc_kernels.cuh — the per-stage kernels of the CUMC3D hot path.
+//
+// One SSP-RK3 stage (solver/rungekutta.f90:38-66) runs as
+//   k_sweep<x>, k_sweep<y>, k_sweep<z>   face fluxes (GET_FLUXES interpolate + RIEMANN)
+//   k_emf                                edge EMFs (GET_FLUXES EMF sums + flux_ct ecell/ecorn)
+//   k_combine                            flux difference + sources + CT curl + RK combine
+//   k_utop                               FROMUTORVE, CUSTOM_CHECKRHO, FROMRVETOU, UPDATE (interior)
+//   k_boundary                           BOUNDARY (+CUSTOM_BOUNDARY) and UPDATE on the ghosts
+// The reference's intermediates primL/primR/consL/consR/fluxL/fluxR/l_rk/sc/
+// ecell never reach HBM here; only the face fluxes and edge EMFs do.
+#pragma once
+#include "cumc_device.cuh"
+
+namespace cumc {
+
+struct Prim {          // stage-start primitive state (with ghosts)
+    const double* w[5];  // rho, vx, vy, vz, p
+    const double* bc[3]; // cell-centred B (bcell)
+    const double* bf[3]; // face B (prim(ibx:ibz) == cons(ibx:ibz))
+};
+
+struct FaceFlux {      // fluxes of one direction, stored at the index of the face's left cell
+    double* f[7];      // rho, mx, my, mz, E, B_t(first in x,y,z order), B_t(second)
+};
+
+struct Cons {
+    double* u[8];
+};
+
+// ----------------------------------------------------------------------------
+// k_sweep: HLL fluxes on the faces of one direction.
+// Faces: normal index 0:n_d, transverse 0:n+1 (solver/spatial.f90:157-168,
+// 235-246, 313-324). Each thread owns one face; it reconstructs the 5 hydro
+// primitives and the 2 transverse cell-centred fields of the two adjacent
+// cells (INTERPOLATE, solver/spatial.f90:131-154) and solves the Riemann
+// problem (HLL_SOLVER).
+// ----------------------------------------------------------------------------
+template <int DIR, int RECON>
+__global__ void __launch_bounds__(128) k_sweep(Box b, Tabs T, Prim pr, double ggas, FaceFlux out) {
+    const int n0 = (DIR == 0 ? b.nx : b.nx + 1) + 1;
+    const int n1 = (DIR == 1 ? b.ny : b.ny + 1) + 1;
+    const int n2 = (DIR == 2 ? b.nz : b.nz + 1) + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total || (b.skip && *b.skip)) return;
+    const int j = (int)(t % n0);
+    const int k = (int)((t / n0) % n1);
+    const int l = (int)(t / ((long long)n0 * n1));
+    const int base = b.idx(j, k, l);
+    const int s = DIR == 0 ? 1 : DIR == 1 ? b.SX : b.SX * b.SY;
+    const int c = DIR == 0 ? j : DIR == 1 ? k : l;  // face between cell c and c+1
+    const AxisTabs A = T.ax[DIR];
+
+    // variables reconstructed along DIR, in natural order
+    constexpr int bt_a = DIR == 0 ? 1 : 0;  // first transverse field component
+    constexpr int bt_b = DIR == 2 ? 1 : 2;  // second transverse field component
+    const double* src[7] = {pr.w[0], pr.w[1], pr.w[2], pr.w[3], pr.w[4], pr.bc[bt_a], pr.bc[bt_b]};
+    const int slot[7] = {IRHO, IVX, IVY, IVZ, ITAU, IBX + bt_a, IBX + bt_b};
+
+    double wl[8], wr[8];
+#pragma unroll
+    for (int v = 0; v < 7; ++v) {
+        const double* q = src[v] + base;
+        double w[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) w[m] = q[(m - 2) * s];  // cells c-2 .. c+3
+        double left, right;
+        if (RECON == 4) {
+            const double d1 = ppm_slope(w[0], w[1], w[2], A.s0[c - 1], A.s1[c - 1]);
+            const double d2 = ppm_slope(w[1], w[2], w[3], A.s0[c], A.s1[c]);
+            const double d3 = ppm_slope(w[2], w[3], w[4], A.s0[c + 1], A.s1[c + 1]);
+            const double d4 = ppm_slope(w[3], w[4], w[5], A.s0[c + 2], A.s1[c + 2]);
+            const double f0 = ppm_face(w[1], w[2], d1, d2, A.a0[c - 1], A.a1[c - 1], A.a2[c - 1], A.a3[c - 1]);
+            const double f1 = ppm_face(w[2], w[3], d2, d3, A.a0[c], A.a1[c], A.a2[c], A.a3[c]);
+            const double f2 = ppm_face(w[3], w[4], d3, d4, A.a0[c + 1], A.a1[c + 1], A.a2[c + 1], A.a3[c + 1]);
+            double vm, vp;
+            ppm_fix(w[2], f0, f1, vm, vp);
+            left = vp;   // primL at face c = vp_out of cell c
+            ppm_fix(w[3], f1, f2, vm, vp);
+            right = vm;  // primR at face c = vm_out of cell c+1
+        } else {
+            const double sl = tvd_slope(w[1], w[2], w[3], A.tcf[c], A.tcb[c]);
+            const double sr = tvd_slope(w[2], w[3], w[4], A.tcf[c + 1], A.tcb[c + 1]);
+            left = w[2] + 0.5 * sl;
+            right = w[3] - 0.5 * sr;
+        }
+        wl[slot[v]] = left;
+        wr[slot[v]] = right;
+    }
+    // normal field: the shared face value (solver/spatial.f90:148-149)
+    const double bn = pr.bf[DIR][base];
+    wl[IBX + DIR] = bn;
+    wr[IBX + DIR] = bn;
+
+    double fx[8];
+    hll_flux<DIR>(wl, wr, ggas, fx);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) out.f[i][base] = fx[i];
+    out.f[5][base] = fx[IBX + bt_a];
+    out.f[6][base] = fx[IBX + bt_b];
+}
+
+// ----------------------------------------------------------------------------
+// k_emf: edge EMFs on 0:n (solver/spatial.f90:190-203,268-281,346-359 then
+// solver/mhd.f90:95-125). ecorn is accumulated in the reference's sweep
+// order starting from zero, then ecorn = 2*ecorn - average of the four cell
+// EMFs E = -v x B.
+// ----------------------------------------------------------------------------
+struct EdgeE {
+    double* e[3];
+};
+
+__device__ __forceinline__ double ecell_x(const Prim& p, int i) { return p.w[3][i] * p.bc[1][i] - p.w[2][i] * p.bc[2][i]; }
+__device__ __forceinline__ double ecell_y(const Prim& p, int i) { return p.w[1][i] * p.bc[2][i] - p.w[3][i] * p.bc[0][i]; }
+__device__ __forceinline__ double ecell_z(const Prim& p, int i) { return p.w[2][i] * p.bc[0][i] - p.w[1][i] * p.bc[1][i]; }
+
+__global__ void __launch_bounds__(256) k_emf(Box b, Prim pr, FaceFlux fx, FaceFlux fy, FaceFlux fz, EdgeE out) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total || (b.skip && *b.skip)) return;
+    const int j = (int)(t % n0);
+    const int k = (int)((t / n0) % n1);
+    const int l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
+    // x-faces carry (by, bz) fluxes, y-faces (bx, bz), z-faces (bx, by)
+    const double* Fx_by = fx.f[5]; const double* Fx_bz = fx.f[6];
+    const double* Fy_bx = fy.f[5]; const double* Fy_bz = fy.f[6];
+    const double* Fz_bx = fz.f[5]; const double* Fz_by = fz.f[6];
+    double ex = 0.0 + 0.25 * (-Fy_bz[i] - Fy_bz[i + sl]);
+    ex = ex + 0.25 * (Fz_by[i] + Fz_by[i + sk]);
+    double ey = 0.0 + 0.25 * (Fx_bz[i] + Fx_bz[i + sl]);
+    ey = ey + 0.25 * (-Fz_bx[i] - Fz_bx[i + sj]);
+    double ez = 0.0 + 0.25 * (-Fx_by[i] - Fx_by[i + sk]);
+    ez = ez + 0.25 * (Fy_bx[i] + Fy_bx[i + sj]);
+    ex = ex * 2.0 - 0.25 * (((ecell_x(pr, i) + ecell_x(pr, i + sl)) + ecell_x(pr, i + sk)) + ecell_x(pr, i + sk + sl));
+    ey = ey * 2.0 - 0.25 * (((ecell_y(pr, i) + ecell_y(pr, i + sl)) + ecell_y(pr, i + sj)) + ecell_y(pr, i + sj + sl));
+    ez = ez * 2.0 - 0.25 * (((ecell_z(pr, i) + ecell_z(pr, i + sk)) + ecell_z(pr, i + sj)) + ecell_z(pr, i + sj + sk));
+    out.e[0][i] = ex;
+    out.e[1][i] = ey;
+    out.e[2][i] = ez;
+}
+
+// ----------------------------------------------------------------------------
+// k_combine: l_rk and the RK stage combine on (0:n)^3 (solver/rungekutta.f90
+// :41-51,75-85,109-119). Hydro l_rk (interior only) is the x, y, z flux
+// differences in that order plus the source (solver/spatial.f90:171-187,
+// 365-375); the field l_rk is the CT curl (solver/mhd.f90:130-153).
+// STAGE 0 stores l_rk instead of combining (SPATIAL alone).
+// ----------------------------------------------------------------------------
+struct CombineArgs {
+    const double* u0[8];  // u_old
+    const double* uc[8];  // cons entering the combine (stages 2 and 3)
+    double* ud[8];        // result (may alias u0 or uc: pointwise)
+    double* lrk[8];       // STAGE 0 output
+    const double* dt;     // device scalar
+    const double* ecorn[3];
+    int geom_repeat;
+    double rho_floor, r_sh;
+};
+
+template <int COORD, int MODEL, int STAGE>
+__global__ void __launch_bounds__(256) k_combine(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy, FaceFlux fz,
+                                                 CombineArgs a) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total || (b.skip && *b.skip)) return;
+    const int j = (int)(t % n0);
+    const int k = (int)((t / n0) % n1);
+    const int l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
+
+    double L[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) L[q] = 0.0;
+
+    if (j >= 1 && k >= 1 && l >= 1) {
+        double gp, gc, gm;
+        geom_flux<COORD, 0>(T, j, k, l, gp, gc, gm);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) L[q] = L[q] - (fx.f[q][i] * gp - fx.f[q][i - sj] * gm) / gc;
+        geom_flux<COORD, 1>(T, j, k, l, gp, gc, gm);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) L[q] = L[q] - (fy.f[q][i] * gp - fy.f[q][i - sk] * gm) / gc;
+        geom_flux<COORD, 2>(T, j, k, l, gp, gc, gm);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) L[q] = L[q] - (fz.f[q][i] * gp - fz.f[q][i - sl] * gm) / gc;
+
+        // source terms sc (solver/spatial.f90:75-102 and CUSTOM_SOURCE)
+        double sc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        const double rho = pr.w[0][i], vx = pr.w[1][i], vy = pr.w[2][i], vz = pr.w[3][i], p = pr.w[4][i];
+        const double bx = pr.bc[0][i], by = pr.bc[1][i], bz = pr.bc[2][i];
+        const double x = T.ax[0].c[j];
+        if (COORD == 2) {  // GEOM_SOURCE cylindrical (solver/coords.f90:127-136)
+            const double bsquare = (bx * bx + by * by) + bz * bz;
+            for (int r = 0; r < a.geom_repeat; ++r) {
+                sc[IVX] = sc[IVX] + (((p + (rho * vy) * vy) + 0.5 * bsquare) - by * by) / (x);
+                sc[IVY] = sc[IVY] - ((rho * vx) * vy - bx * by) / (x);
+            }
+        } else if (COORD == 3) {  // GEOM_SOURCE spherical (solver/coords.f90:139-161)
+            const double bsquare = (bx * bx + by * by) + bz * bz;
+            const double tany = T.tanc[k];
+            for (int r = 0; r < a.geom_repeat; ++r) {
+                sc[IVX] = sc[IVX] + ((2.0 * p + bx * bx) + rho * (vy * vy + vz * vz)) / (x);
+                sc[IVY] = (sc[IVY] + (((p + (rho * vz) * vz) + 0.5 * bsquare) - bz * bz) / (x * tany)) -
+                          ((rho * vx) * vy - bx * by) / (x);
+                sc[IVZ] = (sc[IVZ] - ((rho * vx) * vz - bx * bz) / (x)) - ((rho * vy) * vz - by * bz) / (x * tany);
+            }
+        }
+        if (MODEL == 2) {  // point-mass gravity (model/torus_sph/src/custom.f90:132-146)
+            const double diff = rho - a.rho_floor;
+            const double factor = fmax(copysign(1.0, diff), 0.0);
+            const double dphidr = 1.0 / ((x - a.r_sh) * (x - a.r_sh));
+            sc[IVX] = sc[IVX] + (((-factor) * rho) * dphidr);
+            sc[ITAU] = sc[ITAU] + ((((-factor) * rho) * vx) * dphidr);
+        } else if (MODEL == 3) {  // gravity in (R, z) (model/torus_cyn/src/custom.f90)
+            const double z = T.ax[2].c[l];
+            const double diff = rho - a.rho_floor;
+            const double factor = fmax(copysign(1.0, diff), 0.0);
+            const double radius = sqrt(x * x + z * z);
+            const double dphidr = (x / radius) / ((radius - a.r_sh) * (radius - a.r_sh));
+            const double dphidz = (z / radius) / ((radius - a.r_sh) * (radius - a.r_sh));
+            sc[IVX] = sc[IVX] + (((-factor) * rho) * dphidr);
+            sc[IVZ] = sc[IVZ] + (((-factor) * rho) * dphidz);
+            sc[ITAU] = sc[ITAU] + (((-factor) * rho) * (vx * dphidr + vz * dphidz));
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) L[q] = L[q] + sc[q];
+    }
+
+    // CT update of the face fields (solver/mhd.f90:137-148)
+    {
+        CTf g;
+        geom_ct<COORD>(T, j, k, l, g);
+        const double* Ex = a.ecorn[0];
+        const double* Ey = a.ecorn[1];
+        const double* Ez = a.ecorn[2];
+        L[IBX] = -((Ez[i] * g.bx_ez_p - Ez[i - sk] * g.bx_ez_m) / g.bx_ez_c -
+                   (Ey[i] * g.bx_ey_p - Ey[i - sl] * g.bx_ey_m) / g.bx_ey_c);
+        L[IBY] = -((Ex[i] * g.by_ex_p - Ex[i - sl] * g.by_ex_m) / g.by_ex_c -
+                   (Ez[i] * g.by_ez_p - Ez[i - sj] * g.by_ez_m) / g.by_ez_c);
+        L[IBZ] = -((Ey[i] * g.bz_ey_p - Ey[i - sj] * g.bz_ey_m) / g.bz_ey_c -
+                   (Ex[i] * g.bz_ex_p - Ex[i - sk] * g.bz_ex_m) / g.bz_ex_c);
+    }
+
+    if (STAGE == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) a.lrk[q][i] = L[q];
+        return;
+    }
+    const double dt = *a.dt;
+    constexpr double rk20 = 3.0 / 4.0, rk21 = 1.0 / 4.0, rk22 = 1.0 / 4.0;
+    constexpr double rk30 = 1.0 / 3.0, rk31 = 2.0 / 3.0, rk32 = 2.0 / 3.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const double u0 = a.u0[q][i];
+        double r;
+        if (STAGE == 1) r = u0 + dt * L[q];
+        else if (STAGE == 2) r = (rk20 * u0 + rk21 * a.uc[q][i]) + (rk22 * dt) * L[q];
+        else r = (rk30 * u0 + rk31 * a.uc[q][i]) + (rk32 * dt) * L[q];
+        a.ud[q][i] = r;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// k_utop: on (0:n)^3, FROMUTORVE (solver/fromrvetou.f90:75-127, UtoP_MHD
+// solver/utop.f90:33-68), CUSTOM_CHECKRHO (interior), FROMRVETOU's P_to_U
+// (solver/ptou.f90:33-66) and UPDATE's pressure on the interior
+// (solver/update.f90:27-35). FROM_CONS=false is initial_update: the
+// primitives come from the uploaded model instead of from cons.
+// ----------------------------------------------------------------------------
+struct UtopArgs {
+    double* u[8];       // cons: read, hydro part rewritten
+    double* w[5];       // rho, vx, vy, vz, p
+    double* bc[3];
+    double* eps;
+    double ggas, rho_floor, eps_floor;
+    unsigned int* flag;  // bit 0: non-finite value seen
+};
+
+template <int MODEL, bool FROM_CONS>
+__global__ void __launch_bounds__(256) k_utop(Box b, UtopArgs a) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total || (b.skip && *b.skip)) return;
+    const int j = (int)(t % n0);
+    const int k = (int)((t / n0) % n1);
+    const int l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const bool interior = j >= 1 && k >= 1 && l >= 1;
+
+    double bx, by, bz;
+    if (interior) {  // bcell from the face fields (solver/fromrvetou.f90:97-107, 40-50)
+        bx = 0.5 * (a.u[IBX][i] + a.u[IBX][i - 1]);
+        by = 0.5 * (a.u[IBY][i] + a.u[IBY][i - b.SX]);
+        bz = 0.5 * (a.u[IBZ][i] + a.u[IBZ][i - b.SX * b.SY]);
+        a.bc[0][i] = bx;
+        a.bc[1][i] = by;
+        a.bc[2][i] = bz;
+    } else {
+        bx = a.bc[0][i];
+        by = a.bc[1][i];
+        bz = a.bc[2][i];
+    }
+    const double bsquare = (bx * bx + by * by) + bz * bz;
+    double rho, vx, vy, vz, e;
+    if (FROM_CONS) {
+        rho = a.u[IRHO][i];
+        vx = a.u[IVX][i] / rho;
+        vy = a.u[IVY][i] / rho;
+        vz = a.u[IVZ][i] / rho;
+        const double vsquare = (vx * vx + vy * vy) + vz * vz;
+        e = (a.u[ITAU][i] - 0.5 * bsquare) / rho - 0.5 * vsquare;
+    } else {
+        rho = a.w[0][i];
+        vx = a.w[1][i];
+        vy = a.w[2][i];
+        vz = a.w[3][i];
+        e = a.eps[i];
+    }
+    if (interior) {  // CUSTOM_CHECKRHO
+        if (MODEL == 1) {
+            e = fmax(e, 0.0);
+        } else if (MODEL == 2 || MODEL == 3) {
+            if (rho < a.rho_floor) rho = a.rho_floor;
+            if (e < a.eps_floor) e = a.eps_floor;
+        }
+    }
+    const double vsquare = (vx * vx + vy * vy) + vz * vz;
+    a.u[IRHO][i] = rho;
+    a.u[IVX][i] = vx * rho;
+    a.u[IVY][i] = vy * rho;
+    a.u[IVZ][i] = vz * rho;
+    a.u[ITAU][i] = rho * (e + 0.5 * vsquare) + 0.5 * bsquare;
+    a.w[0][i] = rho;
+    a.w[1][i] = vx;
+    a.w[2][i] = vy;
+    a.w[3][i] = vz;
+    a.eps[i] = e;
+    if (interior) {
+        const double p = (rho * e) * (a.ggas - 1.0);  // EOS_PRESSURE
+        a.w[4][i] = p;
+        if (!(isfinite(p) && isfinite(vsquare) && isfinite(rho))) atomicOr(a.flag, 1u);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// k_boundary: ghost shell of BOUNDARY (solver/boundary.f90:5-13) and UPDATE
+// (solver/update.f90) on the ghosts.
+//
+// The reference fills x, then y, then z ghosts, each pass copying (with the
+// parity signs bfac) from cells the previous passes already filled. Because
+// each pass only reads indices inside 1:n along its own direction, the final
+// value of any ghost equals the product of the three per-direction maps
+// applied to one active cell. Each thread therefore gathers its ghost
+// directly from active cells; no ghost is read, so one launch suffices.
+// Face fields: only the components tangential to a ghost direction are
+// filled (solver/boundary.f90:372-373,472-473,572-573); normal components
+// outside 0:n along their own axis are never read and are left alone.
+// ----------------------------------------------------------------------------
+struct BoundArgs {
+    double* w[5];
+    double* bc[3];
+    double* eps;
+    double* bf[3];
+    int flag[6];            // boundary_flag
+    int eps_yout;           // effective y-outer flag of BOUNDARY1D (solver/boundary.f90:211)
+    signed char fac[6][8];  // bfac_xin, xout, yin, yout, zin, zout (solver/setup.f90:121-230)
+    double ggas;
+};
+
+// source index and sign of one direction's ghost map; returns false if the
+// index is active (identity)
+__device__ __forceinline__ bool gmap(int i, int n, int fin, int fout, int& src, int& side) {
+    if (i < 1) {
+        side = 0;
+        src = fin == 0 ? i + n : fin == 1 ? 1 : 1 - i;
+        return true;
+    }
+    if (i > n) {
+        side = 1;
+        src = fout == 0 ? i - n : fout == 1 ? n : 2 * n + 1 - i;
+        return true;
+    }
+    src = i;
+    side = -1;
+    return false;
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(256) k_boundary(Box b, BoundArgs a) {
+    const long long zsl = 6LL * b.SX * b.SY, ysl = 6LL * b.SX * b.nz, xsl = 6LL * b.ny * b.nz;
+    if (b.skip && *b.skip) return;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int j, k, l;
+    if (t < zsl) {
+        const int s = (int)(t / ((long long)b.SX * b.SY));
+        const int r = (int)(t % ((long long)b.SX * b.SY));
+        l = s < 3 ? s - 2 : b.nz + s - 2;
+        k = r / b.SX - 2;
+        j = r % b.SX - 2;
+    } else if ((t -= zsl) < ysl) {
+        const int s = (int)(t / ((long long)b.SX * b.nz));
+        const int r = (int)(t % ((long long)b.SX * b.nz));
+        k = s < 3 ? s - 2 : b.ny + s - 2;
+        l = r / b.SX + 1;
+        j = r % b.SX - 2;
+    } else if ((t -= ysl) < xsl) {
+        const int s = (int)(t / ((long long)b.ny * b.nz));
+        const int r = (int)(t % ((long long)b.ny * b.nz));
+        j = s < 3 ? s - 2 : b.nx + s - 2;
+        l = r / b.ny + 1;
+        k = r % b.ny + 1;
+    } else {
+        return;
+    }
+    const int i = b.idx(j, k, l);
+    int sj, sk, sl, dj, dk, dl;
+    const bool gx = gmap(j, b.nx, a.flag[0], a.flag[1], sj, dj);
+    const bool gy = gmap(k, b.ny, a.flag[2], a.flag[3], sk, dk);
+    const bool gz = gmap(l, b.nz, a.flag[4], a.flag[5], sl, dl);
+    // parity sign of equation q across the mapped directions (reflecting
+    // boundaries only: flags 0 and 1 copy without sign)
+    auto sgn = [&](int q) -> double {
+        int s = 1;
+        if (gx && a.flag[dj] >= 2) s *= a.fac[dj][q];
+        if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][q];
+        if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][q];
+        return (double)s;
+    };
+    const int src = b.idx(sj, sk, sl);
+    double w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const double v = a.w[q][src];
+        w[q] = (gx && a.flag[dj] >= 2) || (gy && a.flag[2 + dk] >= 2) || (gz && a.flag[4 + dl] >= 2) ? sgn(q) * v : v;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double v = a.bc[q][src];
+        a.bc[q][i] = (gx && a.flag[dj] >= 2) || (gy && a.flag[2 + dk] >= 2) || (gz && a.flag[4 + dl] >= 2)
+                         ? sgn(IBX + q) * v : v;
+    }
+    // eps: BOUNDARY1D with even parity; its y-outer branch keys on flag(3)
+    {
+        int ej = j, ek = k, el = l, dd;
+        gmap(j, b.nx, a.flag[0], a.flag[1], ej, dd);
+        gmap(k, b.ny, a.flag[2], a.eps_yout, ek, dd);
+        gmap(l, b.nz, a.flag[4], a.flag[5], el, dd);
+        const double e = a.eps[b.idx(ej, ek, el)];
+        a.eps[i] = e;
+        // torus ghost clamps (CUSTOM_BOUNDARY) act after all copies
+        if (MODEL == 2 || MODEL == 3) {
+            if (j < 1) w[1] = fmin(w[1], 0.0);
+            if (j > b.nx) w[1] = fmax(w[1], 0.0);
+        }
+        if (MODEL == 3) {
+            if (l < 1) w[3] = fmin(w[3], 0.0);
+            if (l > b.nz) w[3] = fmax(w[3], 0.0);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a.w[q][i] = w[q];
+        a.w[4][i] = (w[0] * e) * (a.ggas - 1.0);  // UPDATE on the ghost
+    }
+    // tangential face fields
+    if (j >= 0 && j <= b.nx && (gy || gz)) {  // Bx: map y and z only
+        int s = 1;
+        if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][IBX];
+        if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][IBX];
+        const double v = a.bf[0][b.idx(j, sk, sl)];
+        a.bf[0][i] = s == 1 ? v : -v;
+    }
+    if (k >= 0 && k <= b.ny && (gx || gz)) {  // By: map x and z only
+        int s = 1;
+        if (gx && a.flag[dj] >= 2) s *= a.fac[dj][IBY];
+        if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][IBY];
+        const double v = a.bf[1][b.idx(sj, k, sl)];
+        a.bf[1][i] = s == 1 ? v : -v;
+    }
+    if (l >= 0 && l <= b.nz && (gx || gy)) {  // Bz: map x and y only
+        int s = 1;
+        if (gx && a.flag[dj] >= 2) s *= a.fac[dj][IBZ];
+        if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][IBZ];
+        const double v = a.bf[2][b.idx(sj, sk, l)];
+        a.bf[2][i] = s == 1 ? v : -v;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// k_finddt: CFL time step (solver/rungekutta.f90:201-261), block min then one
+// 64-bit atomicMin on the (non-negative) bit pattern.
+// ----------------------------------------------------------------------------
+template <int COORD>
+__global__ void __launch_bounds__(256) k_finddt(Box b, Tabs T, Prim pr, double ggas, double cfl,
+                                                unsigned long long* dtmin) {
+    if (b.skip && *b.skip) return;
+    const long long total = (long long)b.nx * b.ny * b.nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double dt_out = 1.0e10;
+    if (t < total) {
+        const int j = (int)(t % b.nx) + 1;
+        const int k = (int)((t / b.nx) % b.ny) + 1;
+        const int l = (int)(t / ((long long)b.nx * b.ny)) + 1;
+        const int i = b.idx(j, k, l);
+        const double rho = pr.w[0][i];
+        const double cs = sqrt((ggas * pr.w[4][i]) / rho);
+        const double a2 = cs * cs;
+        const double a4 = a2 * a2;
+        const double b2x = (pr.bc[0][i] * pr.bc[0][i]) / rho;
+        const double b2y = (pr.bc[1][i] * pr.bc[1][i]) / rho;
+        const double b2z = (pr.bc[2][i] * pr.bc[2][i]) / rho;
+        const double b2 = (b2x + b2y) + b2z;
+        const double b4 = b2 * b2;
+        const double base = (a4 + (2.0 * a2) * b2) + b4;
+        const double cfx = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2x)));
+        const double cfy = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2y)));
+        const double cfz = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2z)));
+        const double lambda = fmax(fmax(fabs(pr.w[1][i]) + cfx, fabs(pr.w[2][i]) + cfy), fabs(pr.w[3][i]) + cfz);
+        double dxl = T.ax[0].d[j], dyl = T.ax[1].d[k], dzl = T.ax[2].d[l];
+        if (COORD == 2) {
+            dyl = T.ax[0].c[j] * dyl;
+        } else if (COORD == 3) {
+            dyl = T.ax[0].c[j] * dyl;
+            dzl = (T.ax[0].c[j] * T.sinc[k]) * dzl;
+        }
+        dt_out = (fmin(fmin(dxl, dyl), dzl) * cfl) / lambda;
+    }
+    // fmin drops NaN, as MIN does for the reference's non-NaN path
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dt_out = fmin(dt_out, __shfl_xor_sync(0xffffffffu, dt_out, o));
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dt_out;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 1.0e10;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0 && v >= 0.0) atomicMin(dtmin, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// ----------------------------------------------------------------------------
+// small device-side scalar kernels for the time loop
+// ----------------------------------------------------------------------------
+struct Clock {
+    double* dt;                // dt used by the stage kernels
+    unsigned long long* dtmin; // finddt result (bit pattern)
+    double* t;                 // simulation time
+    int* steps;                // steps taken
+    int* done;                 // 1 once t >= t_end
+};
+
+__global__ void k_set_scalar(double* p, double v) { *p = v; }
+__global__ void k_reset_dtmin(unsigned long long* p) { *p = (unsigned long long)__double_as_longlong(1.0e10); }
+// loop condition of solver/main.f90:127
+__global__ void k_check_done(Clock c, double t_end) { *c.done = (*c.t < t_end) ? 0 : 1; }
+// dt = finddt, clipped to t_end (solver/main.f90:133-135)
+__global__ void k_clip_dt(Clock c, double t_end) {
+    if (*c.done) return;
+    double dt = __longlong_as_double((long long)*c.dtmin);
+    const double t = *c.t;
+    if (t + dt > t_end) dt = t_end - t;
+    *c.dt = dt;
+}
+__global__ void k_advance_time(Clock c) {
+    if (*c.done) return;
+    *c.t = *c.t + *c.dt;
+    *c.steps = *c.steps + 1;
+}
+
+// ----------------------------------------------------------------------------
+// layout transposes between the reference's AoS arrays and the SoA fields
+// ----------------------------------------------------------------------------
+__global__ void k_aos_to_soa(long long n, int nv, const double* __restrict__ aos, double* const* soa) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    for (int v = 0; v < nv; ++v)
+        if (soa[v]) soa[v][t] = aos[t * nv + v];
+}
+__global__ void k_soa_to_aos(long long n, int nv, double* __restrict__ aos, const double* const* soa) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    for (int v = 0; v < nv; ++v) aos[t * nv + v] = soa[v] ? soa[v][t] : 0.0;
+}
+
+// ----------------------------------------------------------------------------
+// find_divb (solver/mhd.f90:40-52) with GEOM_AREA (solver/coords.f90:173-223):
+// per-block signed max, |div|max and the largest sum of |A B| over a cell's
+// faces, combined on the host.
+// ----------------------------------------------------------------------------
+template <int COORD>
+__global__ void __launch_bounds__(256) k_divb(Box b, Tabs T, const double* bx, const double* by, const double* bz,
+                                              double* part) {
+    const long long total = (long long)b.nx * b.ny * b.nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double smax = -1.0e300, amax = 0.0, fmaxv = 0.0;
+    if (t < total) {
+        const int j = (int)(t % b.nx) + 1;
+        const int k = (int)((t / b.nx) % b.ny) + 1;
+        const int l = (int)(t / ((long long)b.nx * b.ny)) + 1;
+        const int i = b.idx(j, k, l);
+        const double dxl = T.ax[0].d[j], dyl = T.ax[1].d[k], dzl = T.ax[2].d[l];
+        double axp, axm, ayp, aym, azp, azm;
+        if (COORD == 1) {
+            axp = dyl * dzl; axm = dyl * dzl;
+            ayp = dxl * dzl; aym = dxl * dzl;
+            azp = dxl * dyl; azm = dxl * dyl;
+        } else if (COORD == 2) {
+            axp = (T.ax[0].f[j] * dyl) * dzl;
+            axm = (T.ax[0].f[j - 1] * dyl) * dzl;
+            ayp = dxl * dzl; aym = dxl * dzl;
+            azp = T.hr2[j] * dyl; azm = azp;
+        } else {
+            axp = (T.r2[j] * T.dcos[k]) * dzl;
+            axm = (T.r2[j - 1] * T.dcos[k]) * dzl;
+            ayp = (T.hr2[j] * T.sinf[k]) * dzl;
+            aym = (T.hr2[j] * T.sinf[k - 1]) * dzl;
+            azp = T.hr2[j] * dyl; azm = azp;
+        }
+        const double fxp = axp * bx[i], fxm = axm * bx[i - 1];
+        const double fyp = ayp * by[i], fym = aym * by[i - b.SX];
+        const double fzp = azp * bz[i], fzm = azm * bz[i - b.SX * b.SY];
+        const double div = ((fxp - fxm) + (fyp - fym)) + (fzp - fzm);
+        smax = div;
+        amax = fabs(div);
+        fmaxv = ((fabs(fxp) + fabs(fxm)) + (fabs(fyp) + fabs(fym))) + (fabs(fzp) + fabs(fzm));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        smax = fmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+        amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+        fmaxv = fmax(fmaxv, __shfl_xor_sync(0xffffffffu, fmaxv, o));
+    }
+    __shared__ double red[3][32];
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = smax;
+        red[1][threadIdx.x >> 5] = amax;
+        red[2][threadIdx.x >> 5] = fmaxv;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            smax = fmax(smax, red[0][w]);
+            amax = fmax(amax, red[1][w]);
+            fmaxv = fmax(fmaxv, red[2][w]);
+        }
+        part[3 * blockIdx.x + 0] = smax;
+        part[3 * blockIdx.x + 1] = amax;
+        part[3 * blockIdx.x + 2] = fmaxv;
+    }
+}
+
+}  // namespace cumc

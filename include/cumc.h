@@ -1,0 +1,181 @@
+/*
+ * cumc.h — C-ABI of the B200-native CUMC3D hot path.
+ *
+ * The reference (leon-astrophy/CUMPIC, program CUMC3D) drives its per-step
+ * update from solver/main.f90 through argument-free Fortran subroutines that
+ * read and write MODULE DEFINITION globals (solver/definition.f90:238-312).
+ * This header exports the same steps as plain C functions on an opaque
+ * context, so that main.f90 can keep its call sequence through a thin
+ * iso_c_binding module and so that C, C++ and Python
+ * (ctypes) callers can use the same library.
+ *
+ * Conventions
+ *   - Every function returns an int status: CUMC_OK (0) or a CUMC_ERR_* code.
+ *     cumc_last_error() gives a one-line description of the last failure.
+ *   - Host arrays use the reference's Fortran layout: prim/cons are
+ *     REAL*8 A(1:8, -2:nx+3, -2:ny+3, -2:nz+3) (variable index fastest,
+ *     solver/setup.f90:257-260), eps is (-2:nx+3, -2:ny+3, -2:nz+3)
+ *     (solver/setup.f90:263), bcell is (6:8, -2:nx+3, ...) (:286).
+ *     Variable order irho=1, ivx=2, ivy=3, ivz=4, itau=5, ibx=6, iby=7,
+ *     ibz=8 (solver/setup.f90:49-116).  prim(itau) is the gas pressure,
+ *     cons(itau) the total energy; prim/cons(ibx) is the face field at xF(j).
+ *   - The library owns all device memory; caller buffers are never aliased.
+ *   - One host thread per context; calls on a context are serialised on the
+ *     context's own CUDA stream.
+ *   - There is no CPU fallback: if no CUDA device is usable, cumc_init fails.
+ */
+#ifndef CUMC_H
+#define CUMC_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CUMC_OK              0
+#define CUMC_ERR_ARG         1  /* bad pointer or argument value               */
+#define CUMC_ERR_CONFIG      2  /* config rejected (reference would STOP)      */
+#define CUMC_ERR_CUDA        3  /* CUDA runtime error (message has details)    */
+#define CUMC_ERR_NONFINITE   4  /* device flagged NaN/Inf in the evolved state */
+#define CUMC_ERR_STATE       5  /* call made in the wrong order                */
+#define CUMC_ERR_NOMEM       6  /* device allocation failed                    */
+#define CUMC_ERR_LIMIT       7  /* size beyond a documented maximum            */
+
+/* coordinate systems (solver/definition.f90:65-69) */
+#define CUMC_CARTESIAN   1
+#define CUMC_CYLINDRICAL 2
+#define CUMC_SPHERICAL   3
+
+/* reconstruction (solver/definition.f90:158-173); only TVDMM and PPMC are
+ * implemented by the reference (solver/reconstruct.f90:36-49) */
+#define CUMC_TVDMM 1
+#define CUMC_PPMC  4
+
+/* Riemann solver (solver/definition.f90:139-151); the reference implements
+ * HLL only (solver/rsolver.f90:26-34) */
+#define CUMC_HLL 2
+
+/* arithmetic of the path */
+#define CUMC_FP64  0  /* all FP64, bit-compatible with the FP64 restatement  */
+#define CUMC_MIXED 1  /* FP32 reconstruction/HLL/EMF, compensated FP32 state,
+                         FP64 energy and pressure recovery                   */
+
+/* model hooks (model/<m>/src/custom.f90) that sit on the hot path */
+#define CUMC_MODEL_NONE      0  /* all hooks empty                                    */
+#define CUMC_MODEL_RIEMANN   1  /* CUSTOM_CHECKRHO: eps >= 0 (model/riemann/src/custom.f90:54-76) */
+#define CUMC_MODEL_TORUS_SPH 2  /* floors, point-mass gravity, radial no-inflow ghosts
+                                   (model/torus_sph/src/custom.f90:47-150)              */
+#define CUMC_MODEL_TORUS_CYN 3  /* floors, gravity in (R,z), R and z no-inflow ghosts
+                                   (model/torus_cyn/src/custom.f90)                     */
+
+typedef struct cumc_config {
+    int nx, ny, nz;          /* active cells per direction (whole domain on one GPU) */
+    /* face coordinates, nx+7 (ny+7, nz+7) entries for indices -3..n+3
+     * (solver/setup.f90:297-303, filled by GETGRID solver/coords.f90:11-41) */
+    const double *xf, *yf, *zf;
+    int coordinate;          /* CUMC_CARTESIAN / CUMC_CYLINDRICAL / CUMC_SPHERICAL */
+    int boundary_flag[6];    /* x-in, x-out, y-in, y-out, z-in, z-out: 0 periodic,
+                                1 outflow, 2 reflect, 3 axis, 4 equatorial
+                                (solver/definition.f90:74-87)                       */
+    double ggas;             /* adiabatic index (model/<m>/src/defs.f90:14)        */
+    double cfl;              /* Courant number (solver/definition.f90:116)        */
+    int recon;               /* CUMC_PPMC or CUMC_TVDMM                            */
+    int solver;              /* CUMC_HLL                                           */
+    int precision;           /* CUMC_FP64 or CUMC_MIXED                            */
+    int model;               /* CUMC_MODEL_*                                       */
+    double rho_floor;        /* torus models: atmosphere density floor            */
+    double eps_floor;        /* torus models: specific internal energy floor      */
+    double r_sh;             /* torus models: potential softening radius          */
+    /* GET_SOURCE calls GEOM_SOURCE once per equation index imin..imax, so the
+     * geometric source enters 8 times (solver/spatial.f90:86-97).  8 keeps
+     * that behaviour (the default); 1 applies it once. Ignored in Cartesian. */
+    int geom_source_repeat;
+    int reserved[7];         /* must be zero                                      */
+} cumc_config;
+
+typedef struct cumc_ctx cumc_ctx;
+
+/* Replaces POPULATE_DEVICE (solver/openacc.f90:28-59, called at
+ * solver/main.f90:98-100) plus the bfac tables of SETUP_EQNS
+ * (solver/setup.f90:121-230): validates the config, builds the per-axis
+ * metric and reconstruction tables and allocates device state. */
+int cumc_init(const cumc_config* cfg, cumc_ctx** out);
+
+/* Releases every device allocation of the context. */
+int cumc_free(cumc_ctx* ctx);
+
+/* Last error message of this context (ctx may be NULL for cumc_init errors). */
+const char* cumc_last_error(const cumc_ctx* ctx);
+
+/* Host -> device copy of the initial model: prim(1:8,...) and eps(...) in the
+ * Fortran layout, as GET_MODEL leaves them (solver/initial.f90:93). */
+int cumc_upload_state(cumc_ctx* ctx, const double* prim, const double* eps);
+
+/* Device -> host copy replacing "!$ACC UPDATE HOST(prim, eps)"
+ * (solver/dataio.f90:24). Any pointer may be NULL. cons and prim cover the
+ * whole ghosted array; entries the reference never writes are returned as
+ * the library holds them. */
+int cumc_download_state(cumc_ctx* ctx, double* prim, double* cons,
+                        double* eps, double* bcell);
+
+/* initial_update (solver/initial.f90:83-140):
+ * CUSTOM_CHECKRHO -> FROMRVETOU -> BOUNDARY -> UPDATE(0). */
+int cumc_initial_update(cumc_ctx* ctx);
+
+/* finddt (solver/rungekutta.f90:161-265): CFL time step as a device
+ * min-reduction; the value is returned to the host because main.f90 clips
+ * it to total_time (solver/main.f90:133-135). Also reports a non-finite
+ * state flagged by the previous steps (CUMC_ERR_NONFINITE). */
+int cumc_finddt(cumc_ctx* ctx, double* dt);
+
+/* RUNGEKUTTA (solver/rungekutta.f90:12-148): one full SSP-RK3 step with the
+ * given dt, entirely on the device. Returns without a host sync. */
+int cumc_rungekutta(cumc_ctx* ctx, double dt);
+
+/* SPATIAL (solver/spatial.f90:11-68) on the current state: fills the
+ * library's l_rk without advancing. For unit-level checks. */
+int cumc_spatial(cumc_ctx* ctx);
+
+/* Device -> host copy of l_rk(1:8,...) (Fortran layout; entries outside the
+ * ranges SPATIAL writes are zero). */
+int cumc_download_lrk(cumc_ctx* ctx, double* lrk);
+
+/* find_divb (solver/mhd.f90:15-66): *maxdb_signed is the reference's
+ * MAX over cells of the signed, area-weighted divergence; *maxabs_norm is
+ * max |div B| * (cell size) / max|B|, the normalised figure used by the
+ * tests. Either pointer may be NULL. */
+int cumc_divb(cumc_ctx* ctx, double* maxdb_signed, double* maxabs_norm);
+
+/* The time loop of solver/main.f90:127-143 on the device: up to nsteps of
+ * (finddt, clip dt so that t does not pass t_end, RUNGEKUTTA), stopping
+ * early once t reaches t_end. *t_inout is the start time on entry and the
+ * end time on return; *steps_done (may be NULL) gets the steps taken.
+ * dt never leaves the device during the loop; one host sync at the end. */
+int cumc_advance(cumc_ctx* ctx, int nsteps, double t_end, double* t_inout,
+                 int* steps_done);
+
+/* The CUDA stream (cudaStream_t) every call of this context runs on. */
+int cumc_get_stream(cumc_ctx* ctx, void** stream);
+
+/* Per-kernel timing with CUDA events on the context stream. enable=1 starts
+ * recording (and clears totals); cumc_profile_read returns, for kernel class
+ * `which` (CUMC_K_*), the number of launches and their summed milliseconds. */
+#define CUMC_K_SWEEP_X  0
+#define CUMC_K_SWEEP_Y  1
+#define CUMC_K_SWEEP_Z  2
+#define CUMC_K_EMF      3
+#define CUMC_K_COMBINE  4
+#define CUMC_K_UTOP     5
+#define CUMC_K_BOUNDARY 6
+#define CUMC_K_FINDDT   7
+#define CUMC_K_COUNT    8
+int cumc_profile(cumc_ctx* ctx, int enable);
+int cumc_profile_read(cumc_ctx* ctx, int which, int* launches, double* ms);
+
+/* Number of kernel launches the library issued since cumc_init. */
+int cumc_launch_count(cumc_ctx* ctx, long long* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUMC_H */
