@@ -166,12 +166,12 @@ def cpu_reference_rate(n: int, nz: int, steps: int, warmup: int, threads: int | 
     bench resolution (cell size 1/n); returns (Mcell-upd/s, threads, seconds)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from cumpic_b200 import problems as P
-    from _oracle import Oracle, lib as oracle_lib
+    from _oracle import Oracle
 
     threads = threads or os.cpu_count() or 1
     p = P.orszag_tang(n, nz=nz)
     o = Oracle(p, threads=threads)
-    used = oracle_lib().orc_get_threads()
+    used = o._L.orc_get_threads()
     o.upload()
     o.initial_update()
     for _ in range(warmup):

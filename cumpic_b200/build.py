@@ -45,11 +45,16 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
 
 
 def build_oracle(force: bool = False) -> str:
-    """Compile the FP64 CPU oracle (test infrastructure) via oracle/Makefile."""
+    """Compile the FP64 CPU oracle (test infrastructure) via oracle/Makefile,
+    and, where the reference sources are present, the mechanical translation
+    of the reference into oracle/_ref/ (the oracle's own checker)."""
     args = ["make", "-s", "-C", os.path.join(ROOT, "oracle")]
     if force:
         subprocess.run(args + ["clean"], check=True)
     subprocess.run(args, check=True)
+    reference = os.environ.get("CUMC_REFERENCE", "/root/reference")
+    if os.path.isdir(os.path.join(reference, "solver")):
+        subprocess.run(args + ["ref", f"REFERENCE={reference}"], check=True)
     return os.path.join(ROOT, "oracle", "build", "libcumc_oracle.so")
 
 

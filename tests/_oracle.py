@@ -17,16 +17,21 @@ from cumpic_b200.problems import Problem
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_LIB = os.path.join(ROOT, "oracle", "build", "libcumc_oracle.so")
-_LIB = None
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+_LIBS: dict = {}
 
 
-def lib():
-    global _LIB
-    if _LIB is None:
-        if not os.path.exists(ORACLE_LIB):
+def ref_lib_path(model: str) -> str:
+    """mechanical translation of the reference for a model (oracle/f2c_ref.py)"""
+    return os.path.join(REF_DIR, f"libcumc_ref_{model}.so")
+
+
+def lib(path: str = ORACLE_LIB):
+    if path not in _LIBS:
+        if path == ORACLE_LIB and not os.path.exists(ORACLE_LIB):
             from cumpic_b200.build import build_oracle
             build_oracle()
-        L = ctypes.CDLL(ORACLE_LIB)
+        L = ctypes.CDLL(path)
         dp = POINTER(c_double)
         L.orc_create.restype = c_void_p
         L.orc_create.argtypes = [POINTER(N.CumcConfig), c_char_p, c_int]
@@ -41,8 +46,8 @@ def lib():
         L.orc_rungekutta.argtypes = [c_void_p, c_double]
         L.orc_divb.argtypes = [c_void_p, dp]
         L.orc_download.argtypes = [c_void_p, dp, dp, dp, dp, dp]
-        _LIB = L
-    return _LIB
+        _LIBS[path] = L
+    return _LIBS[path]
 
 
 def _dp(a):
@@ -50,9 +55,9 @@ def _dp(a):
 
 
 class Oracle:
-    def __init__(self, problem: Problem, threads: int | None = None):
+    def __init__(self, problem: Problem, threads: int | None = None, lib_path: str = ORACLE_LIB):
         self.problem = problem
-        L = lib()
+        L = self._L = lib(lib_path)
         if threads:
             L.orc_set_threads(int(threads))
         self._cfg = problem.config()
@@ -66,7 +71,7 @@ class Oracle:
 
     def close(self):
         if self._h:
-            lib().orc_free(self._h)
+            self._L.orc_free(self._h)
             self._h = None
 
     def __del__(self):
@@ -83,28 +88,28 @@ class Oracle:
     def upload(self, prim=None, eps=None):
         prim = np.ascontiguousarray(self.problem.prim if prim is None else prim, dtype=np.float64)
         eps = np.ascontiguousarray(self.problem.eps if eps is None else eps, dtype=np.float64)
-        lib().orc_upload(self._h, _dp(prim), _dp(eps))
+        self._L.orc_upload(self._h, _dp(prim), _dp(eps))
 
     def initial_update(self):
-        lib().orc_initial_update(self._h)
+        self._L.orc_initial_update(self._h)
 
     def finddt(self) -> float:
         dt = c_double()
-        lib().orc_finddt(self._h, ctypes.byref(dt))
+        self._L.orc_finddt(self._h, ctypes.byref(dt))
         return dt.value
 
     def rungekutta(self, dt: float):
-        lib().orc_rungekutta(self._h, float(dt))
+        self._L.orc_rungekutta(self._h, float(dt))
 
     def spatial(self) -> np.ndarray:
-        lib().orc_spatial(self._h)
+        self._L.orc_spatial(self._h)
         out = np.zeros(self.shape + (8,))
-        lib().orc_download(self._h, None, None, None, None, _dp(out))
+        self._L.orc_download(self._h, None, None, None, None, _dp(out))
         return out
 
     def find_divb(self) -> float:
         v = c_double()
-        lib().orc_divb(self._h, ctypes.byref(v))
+        self._L.orc_divb(self._h, ctypes.byref(v))
         return v.value
 
     def download(self) -> dict:
@@ -112,7 +117,7 @@ class Oracle:
         cons = np.zeros(self.shape + (8,))
         eps = np.zeros(self.shape)
         bcell = np.zeros(self.shape + (3,))
-        lib().orc_download(self._h, _dp(prim), _dp(cons), _dp(eps), _dp(bcell), None)
+        self._L.orc_download(self._h, _dp(prim), _dp(cons), _dp(eps), _dp(bcell), None)
         return {"prim": prim, "cons": cons, "eps": eps, "bcell": bcell}
 
     def step(self, total_time: float | None = None) -> float:
