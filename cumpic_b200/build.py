@@ -14,12 +14,15 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcumc_b200.so")
 
-NVCC_FLAGS = [
-    "-gencode", "arch=compute_100a,code=sm_100a",
-    "-lineinfo", "-O3", "-std=c++17", "--fmad=false",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-    "-shared",
-]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
+# FP64 path: no multiply-add contraction, IEEE division and square root, so
+# that results are bit-compatible with the FP64 restatement of the reference.
+FP64_FLAGS = ["--fmad=false"]
+# mixed path: FMA and fast FP32 division/square root (FP64 parts stay IEEE).
+MIXED_FLAGS = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]
+UNITS = {"cumc_api.cu": FP64_FLAGS, "cumc_mixed.cu": MIXED_FLAGS}
+NVCC_FLAGS = COMMON + FP64_FLAGS  # flags of the FP64 unit (kept for tools that print them)
 
 
 def _sources():
@@ -36,7 +39,17 @@ def _stale(target, deps):
 
 def build_library(force: bool = False, verbose: bool = False) -> str:
     if force or _stale(LIB, _sources()):
-        cmd = ["nvcc", *NVCC_FLAGS, "-o", LIB + ".tmp", os.path.join(CSRC, "cumc_api.cu")]
+        objdir = os.path.join(HERE, "_build")
+        os.makedirs(objdir, exist_ok=True)
+        objs = []
+        for unit, flags in UNITS.items():
+            obj = os.path.join(objdir, unit.replace(".cu", ".o"))
+            cmd = ["nvcc", *COMMON, *flags, "-c", "-o", obj, os.path.join(CSRC, unit)]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+            objs.append(obj)
+        cmd = ["nvcc", *ARCH, "-shared", "-o", LIB + ".tmp", *objs]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

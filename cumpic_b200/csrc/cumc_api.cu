@@ -6,10 +6,13 @@
 // solver/main.f90:127-143 as a CUDA graph.
 #include "../../include/cumc.h"
 #include "cumc_kernels.cuh"
+#include "cumc_sweep.cuh"
+#include "cumc_mixed.h"
 
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -65,6 +68,10 @@ struct cumc_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     double graph_t_end = 0.0;
     long long graph_launches_per_step = 0;
+    bool sweep_simple = false;  // CUMC_SWEEP=simple selects the one-thread-per-face sweep
+    bool mixed = false;         // CUMC_MIXED: state and kernels of cumc_mixed.cu
+    MixedBufs mb{};
+    MixedParams mp{};
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];
@@ -166,16 +173,53 @@ void build_axis(const double* fsrc, int n, std::vector<double>& out, size_t off,
 // ---------------------------------------------------------------------------
 // stage sequence
 // ---------------------------------------------------------------------------
+template <typename K, typename... Args>
+void launch_grid(cumc_ctx* c, int cls, dim3 grid, int block, size_t smem, K kern, Args... args) {
+    if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
+    ProfEvent pe{cls, nullptr, nullptr};
+    const bool rec = c->prof_on && cls >= 0;
+    if (rec) {
+        cudaEventCreate(&pe.a);
+        cudaEventCreate(&pe.b);
+        cudaEventRecord(pe.a, c->stream);
+    }
+    kern<<<grid, block, smem, c->stream>>>(args...);
+    ++c->launches;
+    if (rec) {
+        cudaEventRecord(pe.b, c->stream);
+        c->prof.push_back(pe);
+    }
+}
+
 template <int DIR>
 void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
     FaceFlux out;
     for (int q = 0; q < 7; ++q) out.f[q] = c->F[DIR][q];
-    const long long n = (long long)((DIR == 0 ? b.nx : b.nx + 1) + 1) * ((DIR == 1 ? b.ny : b.ny + 1) + 1) *
-                        ((DIR == 2 ? b.nz : b.nz + 1) + 1);
+    if (c->sweep_simple) {  // one thread per face, no sharing between faces
+        const long long n = (long long)((DIR == 0 ? b.nx : b.nx + 1) + 1) * ((DIR == 1 ? b.ny : b.ny + 1) + 1) *
+                            ((DIR == 2 ? b.nz : b.nz + 1) + 1);
+        if (c->recon == CUMC_PPMC)
+            launch(c, CUMC_K_SWEEP_X + DIR, n, 128, k_sweep<DIR, 4>, b, c->tabs, pr, c->ggas, out);
+        else
+            launch(c, CUMC_K_SWEEP_X + DIR, n, 128, k_sweep<DIR, 1>, b, c->tabs, pr, c->ggas, out);
+        return;
+    }
+    const dim3 grid = sweep_grid<DIR>(b);
     if (c->recon == CUMC_PPMC)
-        launch(c, CUMC_K_SWEEP_X + DIR, n, 128, k_sweep<DIR, 4>, b, c->tabs, pr, c->ggas, out);
+        launch_grid(c, CUMC_K_SWEEP_X + DIR, grid, SW_THREADS, sw_smem<double>(), k_sweep_tile<DIR, 4, double>, b, c->tabs, pr, c->ggas, out);
     else
-        launch(c, CUMC_K_SWEEP_X + DIR, n, 128, k_sweep<DIR, 1>, b, c->tabs, pr, c->ggas, out);
+        launch_grid(c, CUMC_K_SWEEP_X + DIR, grid, SW_THREADS, sw_smem<double>(), k_sweep_tile<DIR, 1, double>, b, c->tabs, pr, c->ggas, out);
+}
+
+int sweep_attributes(cumc_ctx* c) {
+    const void* k[6] = {(const void*)k_sweep_tile<0, 4, double>, (const void*)k_sweep_tile<1, 4, double>,
+                        (const void*)k_sweep_tile<2, 4, double>, (const void*)k_sweep_tile<0, 1, double>,
+                        (const void*)k_sweep_tile<1, 1, double>, (const void*)k_sweep_tile<2, 1, double>};
+    for (const void* f : k) {
+        cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw_smem<double>());
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaFuncSetAttribute(sweep smem)");
+    }
+    return CUMC_OK;
 }
 
 template <int COORD, int MODEL>
@@ -234,9 +278,9 @@ void boundary(cumc_ctx* c, const Box& b, double* const* u) {
     a.ggas = c->ggas;
     const long long n = 6LL * b.SX * b.SY + 6LL * b.SX * b.nz + 6LL * b.ny * b.nz;
     switch (c->model) {
-        case CUMC_MODEL_TORUS_SPH: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<2>, b, a); break;
-        case CUMC_MODEL_TORUS_CYN: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<3>, b, a); break;
-        default: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<0>, b, a); break;
+        case CUMC_MODEL_TORUS_SPH: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<2, double>, b, a); break;
+        case CUMC_MODEL_TORUS_CYN: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<3, double>, b, a); break;
+        default: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<0, double>, b, a); break;
     }
 }
 
@@ -248,9 +292,31 @@ Prim make_prim(cumc_ctx* c, double* const* u) {
     return p;
 }
 
+// launch hooks for the mixed-path kernels: per-kernel events and launch count
+void mx_pre(void* u, int cls) {
+    auto* c = static_cast<cumc_ctx*>(u);
+    if (c->prof_on && cls >= 0) {
+        ProfEvent pe{cls, nullptr, nullptr};
+        cudaEventCreate(&pe.a);
+        cudaEventCreate(&pe.b);
+        cudaEventRecord(pe.a, c->stream);
+        c->prof.push_back(pe);
+    }
+}
+void mx_post(void* u, int cls) {
+    auto* c = static_cast<cumc_ctx*>(u);
+    ++c->launches;
+    if (c->prof_on && cls >= 0) cudaEventRecord(c->prof.back().b, c->stream);
+}
+Launcher mx_launcher(cumc_ctx* c) { return Launcher{c->stream, mx_pre, mx_post, c}; }
+
 // One SPATIAL + combine + conversions + boundary (solver/rungekutta.f90:38-66).
 // stage 0: SPATIAL only, l_rk stored in c->L.
 void run_stage(cumc_ctx* c, const Box& b, int stage) {
+    if (c->mixed) {
+        if (stage > 0) mixed_stage(mx_launcher(c), b, c->tabs, c->mb, c->mp, stage);
+        return;
+    }
     double* const* Un = c->U[c->cur];
     double* const* Ua = c->U[1 - c->cur];
     double* const* src = (stage <= 1) ? Un : Ua;  // arrays holding prim(ibx:ibz) this stage
@@ -263,7 +329,7 @@ void run_stage(cumc_ctx* c, const Box& b, int stage) {
         for (int q = 0; q < 7; ++q) ff[d].f[q] = c->F[d][q];
     EdgeE ee;
     for (int q = 0; q < 3; ++q) ee.e[q] = c->E[q];
-    launch(c, CUMC_K_EMF, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_emf, b, pr, ff[0], ff[1], ff[2], ee);
+    launch(c, CUMC_K_EMF, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_emf<double>, b, pr, ff[0], ff[1], ff[2], ee);
 
     CombineArgs a{};
     double* const* dst = stage == 1 ? Ua : stage == 2 ? Ua : Un;
@@ -296,6 +362,10 @@ void rk_step(cumc_ctx* c, const Box& b) {
 
 void finddt_launch(cumc_ctx* c, const Box& b) {
     launch(c, -1, 1, 1, k_reset_dtmin, c->dtmin);
+    if (c->mixed) {
+        mixed_finddt(mx_launcher(c), b, c->tabs, c->mb, c->mp, c->dtmin);
+        return;
+    }
     const Prim pr = make_prim(c, c->U[c->cur]);
     const long long n = (long long)b.nx * b.ny * b.nz;
     switch (c->coord) {
@@ -358,7 +428,6 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     if (cfg->recon != CUMC_PPMC && cfg->recon != CUMC_TVDMM) return bad("recon must be CUMC_PPMC or CUMC_TVDMM (the reference implements no other)");
     if (cfg->solver != CUMC_HLL) return bad("solver must be CUMC_HLL (the reference implements no other)");
     if (cfg->precision != CUMC_FP64 && cfg->precision != CUMC_MIXED) return bad("precision must be CUMC_FP64 or CUMC_MIXED");
-    if (cfg->precision == CUMC_MIXED) return bad("CUMC_MIXED is not available in this build");
     if (cfg->model < 0 || cfg->model > 3) return bad("unknown model id");
     for (int i = 0; i < 6; ++i)
         if (cfg->boundary_flag[i] < 0 || cfg->boundary_flag[i] > 4) return bad("boundary_flag entries must be 0..4");
@@ -421,7 +490,18 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
         cumc_free(c);
         return code;
     };
+    int rc;
     if ((e = cudaGetDevice(&c->device)) != cudaSuccess) { cuda_fail(c, e, "cudaGetDevice"); return fail_init(CUMC_ERR_CUDA); }
+    {
+        const char* sw = getenv("CUMC_SWEEP");
+        c->sweep_simple = sw && std::strcmp(sw, "simple") == 0;
+    }
+    if ((rc = sweep_attributes(c)) != CUMC_OK) return fail_init(rc);
+    c->mixed = cfg->precision == CUMC_MIXED;
+    if (c->mixed && (e = mixed_attributes()) != cudaSuccess) {
+        cuda_fail(c, e, "cudaFuncSetAttribute(mixed sweep smem)");
+        return fail_init(CUMC_ERR_CUDA);
+    }
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
         cuda_fail(c, e, "cudaStreamCreate");
         return fail_init(CUMC_ERR_CUDA);
@@ -456,7 +536,6 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     }
     h[offy + 0 * st[1] + 0] = std::sin(cfg->yf[0]);
     double* dtab = nullptr;
-    int rc;
     if ((rc = dalloc(c, &dtab, ntab)) != CUMC_OK) return fail_init(rc);
     if ((e = cudaMemcpy(dtab, h.data(), ntab * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess) {
         cuda_fail(c, e, "table upload");
@@ -483,19 +562,56 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
         if (r != CUMC_OK) return r;
         return cudaMemset(*p, 0, NT * sizeof(double)) == cudaSuccess ? CUMC_OK : CUMC_ERR_CUDA;
     };
-    for (int q = 0; q < 5; ++q) if ((rc = field(&c->w[q])) != CUMC_OK) return fail_init(rc);
-    for (int q = 0; q < 3; ++q) if ((rc = field(&c->bc[q])) != CUMC_OK) return fail_init(rc);
-    if ((rc = field(&c->eps)) != CUMC_OK) return fail_init(rc);
-    for (int s = 0; s < 2; ++s)
-        for (int q = 0; q < 8; ++q) if ((rc = field(&c->U[s][q])) != CUMC_OK) return fail_init(rc);
-    for (int d = 0; d < 3; ++d)
-        for (int q = 0; q < 7; ++q) if ((rc = field(&c->F[d][q])) != CUMC_OK) return fail_init(rc);
-    for (int q = 0; q < 3; ++q) if ((rc = field(&c->E[q])) != CUMC_OK) return fail_init(rc);
+    if (!c->mixed) {
+        for (int q = 0; q < 5; ++q) if ((rc = field(&c->w[q])) != CUMC_OK) return fail_init(rc);
+        for (int q = 0; q < 3; ++q) if ((rc = field(&c->bc[q])) != CUMC_OK) return fail_init(rc);
+        if ((rc = field(&c->eps)) != CUMC_OK) return fail_init(rc);
+        for (int s = 0; s < 2; ++s)
+            for (int q = 0; q < 8; ++q) if ((rc = field(&c->U[s][q])) != CUMC_OK) return fail_init(rc);
+        for (int d = 0; d < 3; ++d)
+            for (int q = 0; q < 7; ++q) if ((rc = field(&c->F[d][q])) != CUMC_OK) return fail_init(rc);
+        for (int q = 0; q < 3; ++q) if ((rc = field(&c->E[q])) != CUMC_OK) return fail_init(rc);
+    } else {
+        auto ffield = [&](float** p) -> int {
+            int r = dalloc(c, p, NT);
+            if (r != CUMC_OK) return r;
+            return cudaMemset(*p, 0, NT * sizeof(float)) == cudaSuccess ? CUMC_OK : CUMC_ERR_CUDA;
+        };
+        MixedBufs& m = c->mb;
+        for (int q = 0; q < 8; ++q) {
+            if (q == ITAU) continue;
+            if ((rc = ffield(&m.uh[q])) != CUMC_OK || (rc = ffield(&m.ul[q])) != CUMC_OK ||
+                (rc = ffield(&m.d[q])) != CUMC_OK)
+                return fail_init(rc);
+        }
+        if ((rc = field(&m.e0)) != CUMC_OK || (rc = field(&m.es)) != CUMC_OK) return fail_init(rc);
+        for (int q = 0; q < 5; ++q) if ((rc = ffield(&m.w[q])) != CUMC_OK) return fail_init(rc);
+        for (int q = 0; q < 3; ++q)
+            if ((rc = ffield(&m.bc[q])) != CUMC_OK || (rc = ffield(&m.bf[q])) != CUMC_OK || (rc = ffield(&m.E[q])) != CUMC_OK)
+                return fail_init(rc);
+        for (int d = 0; d < 3; ++d)
+            for (int q = 0; q < 7; ++q) if ((rc = ffield(&m.F[d][q])) != CUMC_OK) return fail_init(rc);
+        MixedParams& mp = c->mp;
+        mp.ggas = c->ggas;
+        mp.cfl = c->cfl;
+        mp.rho_floor = cfg->rho_floor;
+        mp.eps_floor = cfg->eps_floor;
+        mp.r_sh = cfg->r_sh;
+        for (int i = 0; i < 6; ++i) mp.flag[i] = c->flag[i];
+        mp.eps_yout = c->flag[2] == 0 ? 0 : c->flag[3];
+        std::memcpy(mp.fac, c->fac, sizeof mp.fac);
+        mp.model = c->model;
+        mp.coord = c->coord;
+        mp.recon = c->recon;
+        mp.geom_repeat = c->cfg.geom_source_repeat;
+    }
     if ((rc = dalloc(c, &c->dsoa, 8)) != CUMC_OK) return fail_init(rc);
     if ((rc = dalloc(c, &c->scal, 4)) != CUMC_OK) return fail_init(rc);
     if ((rc = dalloc(c, &c->dtmin, 1)) != CUMC_OK) return fail_init(rc);
     if ((rc = dalloc(c, &c->ints, 4)) != CUMC_OK) return fail_init(rc);
     if ((rc = dalloc(c, &c->flag_dev, 1)) != CUMC_OK) return fail_init(rc);
+    c->mb.dt = c->scal;
+    c->mb.flag = c->flag_dev;
     cudaMemset(c->scal, 0, 4 * sizeof(double));
     cudaMemset(c->ints, 0, 4 * sizeof(int));
     cudaMemset(c->flag_dev, 0, sizeof(unsigned));
@@ -523,7 +639,8 @@ int cumc_free(cumc_ctx* c) {
 // staging buffer for the AoS <-> SoA transposes, allocated on first use
 static int ensure_staging(cumc_ctx* c) {
     if (c->staging) return CUMC_OK;
-    return dalloc(c, &c->staging, 8 * (size_t)c->box.count());
+    // 8 fields in the reference's AoS layout, plus eps for the mixed upload
+    return dalloc(c, &c->staging, 9 * (size_t)c->box.count());
 }
 
 static int put_soa(cumc_ctx* c, const double* host, int nv, double* const* dst) {
@@ -550,6 +667,17 @@ static int get_soa(cumc_ctx* c, double* host, int nv, const double* const* srcp)
 
 int cumc_upload_state(cumc_ctx* c, const double* prim, const double* eps) {
     if (!c || !prim || !eps) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
+    if (c->mixed) {  // kept as FP64 AoS until cumc_initial_update converts it
+        const size_t NT = (size_t)c->box.count();
+        int rc = ensure_staging(c);
+        if (rc != CUMC_OK) return rc;
+        CUMC_CHECK(cudaMemcpyAsync(c->staging, prim, 8 * NT * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CUMC_CHECK(cudaMemcpyAsync(c->staging + 8 * NT, eps, NT * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CUMC_CHECK(cudaStreamSynchronize(c->stream));
+        c->uploaded = true;
+        c->ready = false;
+        return CUMC_OK;
+    }
     double* dst[8] = {c->w[0], c->w[1], c->w[2], c->w[3], c->w[4], c->U[c->cur][IBX], c->U[c->cur][IBY], c->U[c->cur][IBZ]};
     int rc = put_soa(c, prim, 8, dst);
     if (rc != CUMC_OK) return rc;
@@ -564,6 +692,19 @@ int cumc_upload_state(cumc_ctx* c, const double* prim, const double* eps) {
 int cumc_download_state(cumc_ctx* c, double* prim, double* cons, double* eps, double* bcell) {
     if (!c) return CUMC_ERR_ARG;
     int rc;
+    if (c->mixed) {
+        const size_t NT = (size_t)c->box.count();
+        if ((rc = ensure_staging(c)) != CUMC_OK) return rc;
+        double* outs[4] = {prim, cons, eps, bcell};
+        const int nv[4] = {8, 8, 1, 3};
+        for (int w = 0; w < 4; ++w) {
+            if (!outs[w]) continue;
+            mixed_export(mx_launcher(c), c->box, c->mb, c->mp, w, c->staging);
+            CUMC_CHECK(cudaMemcpyAsync(outs[w], c->staging, nv[w] * NT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            CUMC_CHECK(cudaStreamSynchronize(c->stream));
+        }
+        return sync_status(c);
+    }
     double* const* u = c->U[c->cur];
     if (prim) {
         const double* s[8] = {c->w[0], c->w[1], c->w[2], c->w[3], c->w[4], u[IBX], u[IBY], u[IBZ]};
@@ -587,6 +728,12 @@ int cumc_download_state(cumc_ctx* c, double* prim, double* cons, double* eps, do
 int cumc_initial_update(cumc_ctx* c) {
     if (!c) return CUMC_ERR_ARG;
     if (!c->uploaded) return c->fail(CUMC_ERR_STATE, "cumc_upload_state must come first");
+    if (c->mixed) {
+        const size_t NT = (size_t)c->box.count();
+        mixed_initial(mx_launcher(c), c->box, c->tabs, c->mb, c->mp, c->staging, c->staging + 8 * NT);
+        c->ready = true;
+        return sync_status(c);
+    }
     utop(c, c->box, c->U[c->cur], false);
     boundary(c, c->box, c->U[c->cur]);
     c->ready = true;
@@ -620,6 +767,7 @@ int cumc_rungekutta(cumc_ctx* c, double dt) {
 int cumc_spatial(cumc_ctx* c) {
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
+    if (c->mixed) return c->fail(CUMC_ERR_STATE, "cumc_spatial is available for CUMC_FP64 only");
     const size_t NT = (size_t)c->box.count();
     if (!c->L[0])
         for (int q = 0; q < 8; ++q) {
@@ -645,10 +793,18 @@ int cumc_divb(cumc_ctx* c, double* maxdb_signed, double* maxabs_norm) {
     const int nblk = (int)((n + 255) / 256);
     if (!c->divb_part && (rc = dalloc(c, &c->divb_part, 3 * (size_t)nblk)) != CUMC_OK) return rc;
     double* const* u = c->U[c->cur];
+    double* fb[3] = {u[IBX], u[IBY], u[IBZ]};
+    if (c->mixed) {  // face fields as FP64 (hi + lo) in the staging buffer
+        const size_t NT = (size_t)b.count();
+        if ((rc = ensure_staging(c)) != CUMC_OK) return rc;
+        mixed_export(mx_launcher(c), b, c->mb, c->mp, 4, c->staging);
+        for (int q = 0; q < 3; ++q) fb[q] = c->staging + q * NT;
+    }
+    const double *fx = fb[0], *fy = fb[1], *fz = fb[2];
     switch (c->coord) {
-        case CUMC_CARTESIAN: launch(c, -1, n, 256, k_divb<1>, b, c->tabs, (const double*)u[IBX], (const double*)u[IBY], (const double*)u[IBZ], c->divb_part); break;
-        case CUMC_CYLINDRICAL: launch(c, -1, n, 256, k_divb<2>, b, c->tabs, (const double*)u[IBX], (const double*)u[IBY], (const double*)u[IBZ], c->divb_part); break;
-        default: launch(c, -1, n, 256, k_divb<3>, b, c->tabs, (const double*)u[IBX], (const double*)u[IBY], (const double*)u[IBZ], c->divb_part); break;
+        case CUMC_CARTESIAN: launch(c, -1, n, 256, k_divb<1>, b, c->tabs, fx, fy, fz, c->divb_part); break;
+        case CUMC_CYLINDRICAL: launch(c, -1, n, 256, k_divb<2>, b, c->tabs, fx, fy, fz, c->divb_part); break;
+        default: launch(c, -1, n, 256, k_divb<3>, b, c->tabs, fx, fy, fz, c->divb_part); break;
     }
     std::vector<double> h(3 * (size_t)nblk);
     CUMC_CHECK(cudaMemcpyAsync(h.data(), c->divb_part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

@@ -13,15 +13,19 @@
 
 namespace cumc {
 
-struct Prim {          // stage-start primitive state (with ghosts)
-    const double* w[5];  // rho, vx, vy, vz, p
-    const double* bc[3]; // cell-centred B (bcell)
-    const double* bf[3]; // face B (prim(ibx:ibz) == cons(ibx:ibz))
+template <typename R>
+struct PrimT {         // stage-start primitive state (with ghosts), storage type R
+    const R* w[5];     // rho, vx, vy, vz, p
+    const R* bc[3];    // cell-centred B (bcell)
+    const R* bf[3];    // face B (prim(ibx:ibz) == cons(ibx:ibz))
 };
+using Prim = PrimT<double>;
 
-struct FaceFlux {      // fluxes of one direction, stored at the index of the face's left cell
-    double* f[7];      // rho, mx, my, mz, E, B_t(first in x,y,z order), B_t(second)
+template <typename R>
+struct FaceFluxT {     // fluxes of one direction, stored at the index of the face's left cell
+    R* f[7];           // rho, mx, my, mz, E, B_t(first in x,y,z order), B_t(second)
 };
+using FaceFlux = FaceFluxT<double>;
 
 struct Cons {
     double* u[8];
@@ -106,15 +110,22 @@ __global__ void __launch_bounds__(128) k_sweep(Box b, Tabs T, Prim pr, double gg
 // order starting from zero, then ecorn = 2*ecorn - average of the four cell
 // EMFs E = -v x B.
 // ----------------------------------------------------------------------------
-struct EdgeE {
-    double* e[3];
+template <typename R>
+struct EdgeET {
+    R* e[3];
 };
+using EdgeE = EdgeET<double>;
 
-__device__ __forceinline__ double ecell_x(const Prim& p, int i) { return p.w[3][i] * p.bc[1][i] - p.w[2][i] * p.bc[2][i]; }
-__device__ __forceinline__ double ecell_y(const Prim& p, int i) { return p.w[1][i] * p.bc[2][i] - p.w[3][i] * p.bc[0][i]; }
-__device__ __forceinline__ double ecell_z(const Prim& p, int i) { return p.w[2][i] * p.bc[0][i] - p.w[1][i] * p.bc[1][i]; }
+template <typename R>
+__device__ __forceinline__ R ecell_x(const PrimT<R>& p, int i) { return p.w[3][i] * p.bc[1][i] - p.w[2][i] * p.bc[2][i]; }
+template <typename R>
+__device__ __forceinline__ R ecell_y(const PrimT<R>& p, int i) { return p.w[1][i] * p.bc[2][i] - p.w[3][i] * p.bc[0][i]; }
+template <typename R>
+__device__ __forceinline__ R ecell_z(const PrimT<R>& p, int i) { return p.w[2][i] * p.bc[0][i] - p.w[1][i] * p.bc[1][i]; }
 
-__global__ void __launch_bounds__(256) k_emf(Box b, Prim pr, FaceFlux fx, FaceFlux fy, FaceFlux fz, EdgeE out) {
+template <typename R>
+__global__ void __launch_bounds__(256) k_emf(Box b, PrimT<R> pr, FaceFluxT<R> fx, FaceFluxT<R> fy, FaceFluxT<R> fz,
+                                             EdgeET<R> out) {
     const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
     const long long total = (long long)n0 * n1 * n2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -125,18 +136,19 @@ __global__ void __launch_bounds__(256) k_emf(Box b, Prim pr, FaceFlux fx, FaceFl
     const int i = b.idx(j, k, l);
     const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
     // x-faces carry (by, bz) fluxes, y-faces (bx, bz), z-faces (bx, by)
-    const double* Fx_by = fx.f[5]; const double* Fx_bz = fx.f[6];
-    const double* Fy_bx = fy.f[5]; const double* Fy_bz = fy.f[6];
-    const double* Fz_bx = fz.f[5]; const double* Fz_by = fz.f[6];
-    double ex = 0.0 + 0.25 * (-Fy_bz[i] - Fy_bz[i + sl]);
-    ex = ex + 0.25 * (Fz_by[i] + Fz_by[i + sk]);
-    double ey = 0.0 + 0.25 * (Fx_bz[i] + Fx_bz[i + sl]);
-    ey = ey + 0.25 * (-Fz_bx[i] - Fz_bx[i + sj]);
-    double ez = 0.0 + 0.25 * (-Fx_by[i] - Fx_by[i + sk]);
-    ez = ez + 0.25 * (Fy_bx[i] + Fy_bx[i + sj]);
-    ex = ex * 2.0 - 0.25 * (((ecell_x(pr, i) + ecell_x(pr, i + sl)) + ecell_x(pr, i + sk)) + ecell_x(pr, i + sk + sl));
-    ey = ey * 2.0 - 0.25 * (((ecell_y(pr, i) + ecell_y(pr, i + sl)) + ecell_y(pr, i + sj)) + ecell_y(pr, i + sj + sl));
-    ez = ez * 2.0 - 0.25 * (((ecell_z(pr, i) + ecell_z(pr, i + sk)) + ecell_z(pr, i + sj)) + ecell_z(pr, i + sj + sk));
+    const R* Fx_by = fx.f[5]; const R* Fx_bz = fx.f[6];
+    const R* Fy_bx = fy.f[5]; const R* Fy_bz = fy.f[6];
+    const R* Fz_bx = fz.f[5]; const R* Fz_by = fz.f[6];
+    const R q = R(0.25);
+    R ex = R(0) + q * (-Fy_bz[i] - Fy_bz[i + sl]);
+    ex = ex + q * (Fz_by[i] + Fz_by[i + sk]);
+    R ey = R(0) + q * (Fx_bz[i] + Fx_bz[i + sl]);
+    ey = ey + q * (-Fz_bx[i] - Fz_bx[i + sj]);
+    R ez = R(0) + q * (-Fx_by[i] - Fx_by[i + sk]);
+    ez = ez + q * (Fy_bx[i] + Fy_bx[i + sj]);
+    ex = ex * R(2) - q * (((ecell_x(pr, i) + ecell_x(pr, i + sl)) + ecell_x(pr, i + sk)) + ecell_x(pr, i + sk + sl));
+    ey = ey * R(2) - q * (((ecell_y(pr, i) + ecell_y(pr, i + sl)) + ecell_y(pr, i + sj)) + ecell_y(pr, i + sj + sl));
+    ez = ez * R(2) - q * (((ecell_z(pr, i) + ecell_z(pr, i + sk)) + ecell_z(pr, i + sj)) + ecell_z(pr, i + sj + sk));
     out.e[0][i] = ex;
     out.e[1][i] = ey;
     out.e[2][i] = ez;
@@ -362,11 +374,12 @@ __global__ void __launch_bounds__(256) k_utop(Box b, UtopArgs a) {
 // filled (solver/boundary.f90:372-373,472-473,572-573); normal components
 // outside 0:n along their own axis are never read and are left alone.
 // ----------------------------------------------------------------------------
-struct BoundArgs {
-    double* w[5];
-    double* bc[3];
-    double* eps;
-    double* bf[3];
+template <typename R>
+struct BoundArgsT {
+    R* w[5];
+    R* bc[3];
+    double* eps;            // FP64 path: gathered, then p = rho*eps*(ggas-1); mixed path: null, p gathered
+    R* bf[3];
     int flag[6];            // boundary_flag
     int eps_yout;           // effective y-outer flag of BOUNDARY1D (solver/boundary.f90:211)
     signed char fac[6][8];  // bfac_xin, xout, yin, yout, zin, zout (solver/setup.f90:121-230)
@@ -391,8 +404,10 @@ __device__ __forceinline__ bool gmap(int i, int n, int fin, int fout, int& src, 
     return false;
 }
 
-template <int MODEL>
-__global__ void __launch_bounds__(256) k_boundary(Box b, BoundArgs a) {
+using BoundArgs = BoundArgsT<double>;
+
+template <int MODEL, typename R>
+__global__ void __launch_bounds__(256) k_boundary(Box b, BoundArgsT<R> a) {
     const long long zsl = 6LL * b.SX * b.SY, ysl = 6LL * b.SX * b.nz, xsl = 6LL * b.ny * b.nz;
     if (b.skip && *b.skip) return;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -425,67 +440,70 @@ __global__ void __launch_bounds__(256) k_boundary(Box b, BoundArgs a) {
     const bool gz = gmap(l, b.nz, a.flag[4], a.flag[5], sl, dl);
     // parity sign of equation q across the mapped directions (reflecting
     // boundaries only: flags 0 and 1 copy without sign)
-    auto sgn = [&](int q) -> double {
+    // parity sign of equation q across the mapped directions (bfac is 1
+    // except at reflecting faces, flags >= 2)
+    auto sgn = [&](int q) -> int {
         int s = 1;
         if (gx && a.flag[dj] >= 2) s *= a.fac[dj][q];
         if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][q];
         if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][q];
-        return (double)s;
+        return s;
     };
     const int src = b.idx(sj, sk, sl);
-    double w[4];
+    R w[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const double v = a.w[q][src];
-        w[q] = (gx && a.flag[dj] >= 2) || (gy && a.flag[2 + dk] >= 2) || (gz && a.flag[4 + dl] >= 2) ? sgn(q) * v : v;
+        const R v = a.w[q][src];
+        w[q] = sgn(q) == 1 ? v : -v;
     }
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-        const double v = a.bc[q][src];
-        a.bc[q][i] = (gx && a.flag[dj] >= 2) || (gy && a.flag[2 + dk] >= 2) || (gz && a.flag[4 + dl] >= 2)
-                         ? sgn(IBX + q) * v : v;
+        const R v = a.bc[q][src];
+        a.bc[q][i] = sgn(IBX + q) == 1 ? v : -v;
     }
-    // eps: BOUNDARY1D with even parity; its y-outer branch keys on flag(3)
-    {
+    // torus ghost clamps (CUSTOM_BOUNDARY) act after all copies
+    if (MODEL == 2 || MODEL == 3) {
+        if (j < 1) w[1] = fmin(w[1], R(0));
+        if (j > b.nx) w[1] = fmax(w[1], R(0));
+    }
+    if (MODEL == 3) {
+        if (l < 1) w[3] = fmin(w[3], R(0));
+        if (l > b.nz) w[3] = fmax(w[3], R(0));
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a.w[q][i] = w[q];
+    if (a.eps) {
+        // eps: BOUNDARY1D with even parity; its y-outer branch keys on flag(3)
         int ej = j, ek = k, el = l, dd;
         gmap(j, b.nx, a.flag[0], a.flag[1], ej, dd);
         gmap(k, b.ny, a.flag[2], a.eps_yout, ek, dd);
         gmap(l, b.nz, a.flag[4], a.flag[5], el, dd);
         const double e = a.eps[b.idx(ej, ek, el)];
         a.eps[i] = e;
-        // torus ghost clamps (CUSTOM_BOUNDARY) act after all copies
-        if (MODEL == 2 || MODEL == 3) {
-            if (j < 1) w[1] = fmin(w[1], 0.0);
-            if (j > b.nx) w[1] = fmax(w[1], 0.0);
-        }
-        if (MODEL == 3) {
-            if (l < 1) w[3] = fmin(w[3], 0.0);
-            if (l > b.nz) w[3] = fmax(w[3], 0.0);
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) a.w[q][i] = w[q];
-        a.w[4][i] = (w[0] * e) * (a.ggas - 1.0);  // UPDATE on the ghost
+        a.w[4][i] = (R)(((double)w[0] * e) * (a.ggas - 1.0));  // UPDATE on the ghost
+    } else {
+        a.w[4][i] = a.w[4][src];  // pressure is even under every map
     }
     // tangential face fields
     if (j >= 0 && j <= b.nx && (gy || gz)) {  // Bx: map y and z only
         int s = 1;
         if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][IBX];
         if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][IBX];
-        const double v = a.bf[0][b.idx(j, sk, sl)];
+        const R v = a.bf[0][b.idx(j, sk, sl)];
         a.bf[0][i] = s == 1 ? v : -v;
     }
     if (k >= 0 && k <= b.ny && (gx || gz)) {  // By: map x and z only
         int s = 1;
         if (gx && a.flag[dj] >= 2) s *= a.fac[dj][IBY];
         if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][IBY];
-        const double v = a.bf[1][b.idx(sj, k, sl)];
+        const R v = a.bf[1][b.idx(sj, k, sl)];
         a.bf[1][i] = s == 1 ? v : -v;
     }
     if (l >= 0 && l <= b.nz && (gx || gy)) {  // Bz: map x and y only
         int s = 1;
         if (gx && a.flag[dj] >= 2) s *= a.fac[dj][IBZ];
         if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][IBZ];
-        const double v = a.bf[2][b.idx(sj, sk, l)];
+        const R v = a.bf[2][b.idx(sj, sk, l)];
         a.bf[2][i] = s == 1 ? v : -v;
     }
 }
@@ -494,8 +512,8 @@ __global__ void __launch_bounds__(256) k_boundary(Box b, BoundArgs a) {
 // k_finddt: CFL time step (solver/rungekutta.f90:201-261), block min then one
 // 64-bit atomicMin on the (non-negative) bit pattern.
 // ----------------------------------------------------------------------------
-template <int COORD>
-__global__ void __launch_bounds__(256) k_finddt(Box b, Tabs T, Prim pr, double ggas, double cfl,
+template <int COORD, typename R = double>
+__global__ void __launch_bounds__(256) k_finddt(Box b, Tabs T, PrimT<R> pr, double ggas, double cfl,
                                                 unsigned long long* dtmin) {
     if (b.skip && *b.skip) return;
     const long long total = (long long)b.nx * b.ny * b.nz;
@@ -507,19 +525,21 @@ __global__ void __launch_bounds__(256) k_finddt(Box b, Tabs T, Prim pr, double g
         const int l = (int)(t / ((long long)b.nx * b.ny)) + 1;
         const int i = b.idx(j, k, l);
         const double rho = pr.w[0][i];
-        const double cs = sqrt((ggas * pr.w[4][i]) / rho);
+        const double cs = sqrt((ggas * (double)pr.w[4][i]) / rho);
         const double a2 = cs * cs;
         const double a4 = a2 * a2;
-        const double b2x = (pr.bc[0][i] * pr.bc[0][i]) / rho;
-        const double b2y = (pr.bc[1][i] * pr.bc[1][i]) / rho;
-        const double b2z = (pr.bc[2][i] * pr.bc[2][i]) / rho;
+        const double bcx = pr.bc[0][i], bcy = pr.bc[1][i], bcz = pr.bc[2][i];
+        const double b2x = (bcx * bcx) / rho;
+        const double b2y = (bcy * bcy) / rho;
+        const double b2z = (bcz * bcz) / rho;
         const double b2 = (b2x + b2y) + b2z;
         const double b4 = b2 * b2;
         const double base = (a4 + (2.0 * a2) * b2) + b4;
         const double cfx = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2x)));
         const double cfy = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2y)));
         const double cfz = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2z)));
-        const double lambda = fmax(fmax(fabs(pr.w[1][i]) + cfx, fabs(pr.w[2][i]) + cfy), fabs(pr.w[3][i]) + cfz);
+        const double vx = pr.w[1][i], vy = pr.w[2][i], vz = pr.w[3][i];
+        const double lambda = fmax(fmax(fabs(vx) + cfx, fabs(vy) + cfy), fabs(vz) + cfz);
         double dxl = T.ax[0].d[j], dyl = T.ax[1].d[k], dzl = T.ax[2].d[l];
         if (COORD == 2) {
             dyl = T.ax[0].c[j] * dyl;
@@ -554,19 +574,19 @@ struct Clock {
     int* done;                 // 1 once t >= t_end
 };
 
-__global__ void k_set_scalar(double* p, double v) { *p = v; }
-__global__ void k_reset_dtmin(unsigned long long* p) { *p = (unsigned long long)__double_as_longlong(1.0e10); }
+static __global__ void k_set_scalar(double* p, double v) { *p = v; }
+static __global__ void k_reset_dtmin(unsigned long long* p) { *p = (unsigned long long)__double_as_longlong(1.0e10); }
 // loop condition of solver/main.f90:127
-__global__ void k_check_done(Clock c, double t_end) { *c.done = (*c.t < t_end) ? 0 : 1; }
+static __global__ void k_check_done(Clock c, double t_end) { *c.done = (*c.t < t_end) ? 0 : 1; }
 // dt = finddt, clipped to t_end (solver/main.f90:133-135)
-__global__ void k_clip_dt(Clock c, double t_end) {
+static __global__ void k_clip_dt(Clock c, double t_end) {
     if (*c.done) return;
     double dt = __longlong_as_double((long long)*c.dtmin);
     const double t = *c.t;
     if (t + dt > t_end) dt = t_end - t;
     *c.dt = dt;
 }
-__global__ void k_advance_time(Clock c) {
+static __global__ void k_advance_time(Clock c) {
     if (*c.done) return;
     *c.t = *c.t + *c.dt;
     *c.steps = *c.steps + 1;
@@ -575,13 +595,13 @@ __global__ void k_advance_time(Clock c) {
 // ----------------------------------------------------------------------------
 // layout transposes between the reference's AoS arrays and the SoA fields
 // ----------------------------------------------------------------------------
-__global__ void k_aos_to_soa(long long n, int nv, const double* __restrict__ aos, double* const* soa) {
+static __global__ void k_aos_to_soa(long long n, int nv, const double* __restrict__ aos, double* const* soa) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     for (int v = 0; v < nv; ++v)
         if (soa[v]) soa[v][t] = aos[t * nv + v];
 }
-__global__ void k_soa_to_aos(long long n, int nv, double* __restrict__ aos, const double* const* soa) {
+static __global__ void k_soa_to_aos(long long n, int nv, double* __restrict__ aos, const double* const* soa) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     for (int v = 0; v < nv; ++v) aos[t * nv + v] = soa[v] ? soa[v][t] : 0.0;

@@ -1,0 +1,506 @@
+// cumc_mixed.cu — mixed-precision form of the CUMC3D step (CUMC_MIXED).
+//
+// Compiled separately from the FP64 path, with FMA contraction and fast FP32
+// division: nothing here is meant to be bit-compatible with the reference.
+//
+// What runs in which precision:
+//   * reconstruction, HLL fluxes, EMFs, flux differences, sources, CT curl: FP32
+//     (the tiled sweep and k_emf templates shared with the FP64 path);
+//   * the RK3 accumulation of rho, rho v and B: U^n is kept as a hi/lo pair of
+//     FP32 values and updated with Knuth's TwoSum and Dekker's FastTwoSum;
+//     stage states are stored as the FP32 increment d_s = U_s - U^n, so their
+//     rounding error scales with the increment, not with U;
+//   * total energy and its stage combine, and the pressure recovery
+//     p = (g-1) rho ((E - B^2/2)/rho - v^2/2) (solver/utop.f90:63-65), which
+//     cancels catastrophically at low plasma beta: FP64.
+// SSP-RK3 (solver/rungekutta.f90:46,80,114) in increment form:
+//   d1 = dt L1,  d2 = (d1 + dt L2)/4,  U^{n+1} = U^n + 2/3 (d2 + dt L3)
+// which equals u1 = u0 + dt L1, u2 = 3/4 u0 + 1/4 u1 + 1/4 dt L2,
+// u3 = 1/3 u0 + 2/3 u2 + 2/3 dt L3 in exact arithmetic.
+#include "cumc_mixed.h"
+#include "cumc_sweep.cuh"
+
+namespace cumc {
+namespace {
+
+// Knuth's TwoSum: s + e == a + b exactly
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    const float bb = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+// Dekker's FastTwoSum (|a| >= |b|)
+__device__ __forceinline__ void fast_two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    e = __fsub_rn(b, __fsub_rn(s, a));
+}
+// (hi, lo) += x
+__device__ __forceinline__ void df_add(float& hi, float& lo, float x) {
+    float s, e;
+    two_sum(hi, x, s, e);
+    e = __fadd_rn(e, lo);
+    fast_two_sum(s, e, hi, lo);
+}
+__device__ __forceinline__ void df_split(double v, float& hi, float& lo) {
+    hi = __double2float_rn(v);
+    lo = __double2float_rn(v - (double)hi);
+}
+__device__ __forceinline__ double df_val(float hi, float lo) { return (double)hi + (double)lo; }
+
+template <typename K, typename... Args>
+void run(const Launcher& L, int cls, dim3 grid, int block, size_t smem, K kern, Args... args) {
+    if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
+    if (L.pre) L.pre(L.user, cls);
+    kern<<<grid, block, smem, L.stream>>>(args...);
+    if (L.post) L.post(L.user, cls);
+}
+inline dim3 g1(long long n, int block) { return dim3((unsigned)((n + block - 1) / block)); }
+
+// ---------------------------------------------------------------------------
+// flux difference + sources + CT curl in FP32, then the increment-form combine
+// ---------------------------------------------------------------------------
+struct CombineMx {
+    float* uh[8];
+    float* ul[8];
+    double* e0;
+    float* d[8];
+    double* es;
+    const float* w[5];
+    const float* bc[3];
+    const float* ecorn[3];
+    const double* dt;
+    int geom_repeat;
+    float rho_floor, r_sh;
+};
+
+template <int COORD, int MODEL, int STAGE>
+__global__ void __launch_bounds__(256) k_combine_mx(Box b, Tabs T, FaceFluxT<float> fx, FaceFluxT<float> fy,
+                                                    FaceFluxT<float> fz, CombineMx a) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total || (b.skip && *b.skip)) return;
+    const int j = (int)(t % n0);
+    const int k = (int)((t / n0) % n1);
+    const int l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
+    float L[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) L[q] = 0.f;
+    if (j >= 1 && k >= 1 && l >= 1) {
+        double gp, gc, gm;
+        geom_flux<COORD, 0>(T, j, k, l, gp, gc, gm);
+        float fp = (float)gp, fm = (float)gm, fi = (float)(1.0 / gc);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) L[q] -= (fx.f[q][i] * fp - fx.f[q][i - sj] * fm) * fi;
+        geom_flux<COORD, 1>(T, j, k, l, gp, gc, gm);
+        fp = (float)gp; fm = (float)gm; fi = (float)(1.0 / gc);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) L[q] -= (fy.f[q][i] * fp - fy.f[q][i - sk] * fm) * fi;
+        geom_flux<COORD, 2>(T, j, k, l, gp, gc, gm);
+        fp = (float)gp; fm = (float)gm; fi = (float)(1.0 / gc);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) L[q] -= (fz.f[q][i] * fp - fz.f[q][i - sl] * fm) * fi;
+        const float rho = a.w[0][i], vx = a.w[1][i], vy = a.w[2][i], vz = a.w[3][i], p = a.w[4][i];
+        const float bx = a.bc[0][i], by = a.bc[1][i], bz = a.bc[2][i];
+        const float x = (float)T.ax[0].c[j];
+        const float rep = (float)a.geom_repeat;
+        if (COORD == 2) {
+            const float bsq = bx * bx + by * by + bz * bz;
+            L[IVX] += rep * ((p + rho * vy * vy + 0.5f * bsq - by * by) / x);
+            L[IVY] -= rep * ((rho * vx * vy - bx * by) / x);
+        } else if (COORD == 3) {
+            const float bsq = bx * bx + by * by + bz * bz;
+            const float tany = (float)T.tanc[k];
+            L[IVX] += rep * ((2.f * p + bx * bx + rho * (vy * vy + vz * vz)) / x);
+            L[IVY] += rep * ((p + rho * vz * vz + 0.5f * bsq - bz * bz) / (x * tany) - (rho * vx * vy - bx * by) / x);
+            L[IVZ] -= rep * ((rho * vx * vz - bx * bz) / x + (rho * vy * vz - by * bz) / (x * tany));
+        }
+        if (MODEL == 2) {
+            const float factor = rho >= a.rho_floor ? 1.f : 0.f;
+            const float dphidr = 1.f / ((x - a.r_sh) * (x - a.r_sh));
+            L[IVX] -= factor * rho * dphidr;
+            L[ITAU] -= factor * rho * vx * dphidr;
+        } else if (MODEL == 3) {
+            const float z = (float)T.ax[2].c[l];
+            const float factor = rho >= a.rho_floor ? 1.f : 0.f;
+            const float radius = sqrtf(x * x + z * z);
+            const float inv = 1.f / (radius * (radius - a.r_sh) * (radius - a.r_sh));
+            L[IVX] -= factor * rho * x * inv;
+            L[IVZ] -= factor * rho * z * inv;
+            L[ITAU] -= factor * rho * (vx * x + vz * z) * inv;
+        }
+    }
+    {
+        CTf g;
+        geom_ct<COORD>(T, j, k, l, g);
+        const float* Ex = a.ecorn[0];
+        const float* Ey = a.ecorn[1];
+        const float* Ez = a.ecorn[2];
+        L[IBX] = -((Ez[i] * (float)g.bx_ez_p - Ez[i - sk] * (float)g.bx_ez_m) * (float)(1.0 / g.bx_ez_c) -
+                   (Ey[i] * (float)g.bx_ey_p - Ey[i - sl] * (float)g.bx_ey_m) * (float)(1.0 / g.bx_ey_c));
+        L[IBY] = -((Ex[i] * (float)g.by_ex_p - Ex[i - sl] * (float)g.by_ex_m) * (float)(1.0 / g.by_ex_c) -
+                   (Ez[i] * (float)g.by_ez_p - Ez[i - sj] * (float)g.by_ez_m) * (float)(1.0 / g.by_ez_c));
+        L[IBZ] = -((Ey[i] * (float)g.bz_ey_p - Ey[i - sj] * (float)g.bz_ey_m) * (float)(1.0 / g.bz_ey_c) -
+                   (Ex[i] * (float)g.bz_ex_p - Ex[i - sk] * (float)g.bz_ex_m) * (float)(1.0 / g.bz_ex_c));
+    }
+    const double dt = *a.dt;
+    const float dtf = (float)dt;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        if (q == ITAU) continue;
+        if (STAGE == 1) {
+            a.d[q][i] = dtf * L[q];
+        } else if (STAGE == 2) {
+            a.d[q][i] = 0.25f * (a.d[q][i] + dtf * L[q]);
+        } else {
+            const float inc = (2.f / 3.f) * (a.d[q][i] + dtf * L[q]);
+            float hi = a.uh[q][i], lo = a.ul[q][i];
+            df_add(hi, lo, inc);
+            a.uh[q][i] = hi;
+            a.ul[q][i] = lo;
+        }
+    }
+    const double LE = (double)L[ITAU];
+    constexpr double rk20 = 3.0 / 4.0, rk21 = 1.0 / 4.0, rk22 = 1.0 / 4.0;
+    constexpr double rk30 = 1.0 / 3.0, rk31 = 2.0 / 3.0, rk32 = 2.0 / 3.0;
+    if (STAGE == 1) a.es[i] = a.e0[i] + dt * LE;
+    else if (STAGE == 2) a.es[i] = (rk20 * a.e0[i] + rk21 * a.es[i]) + (rk22 * dt) * LE;
+    else a.e0[i] = (rk30 * a.e0[i] + rk31 * a.es[i]) + (rk32 * dt) * LE;
+}
+
+// ---------------------------------------------------------------------------
+// conserved -> primitive with FP64 pressure recovery; floors; FP32 prims out
+// ---------------------------------------------------------------------------
+struct UtopMx {
+    float* uh[8];
+    float* ul[8];
+    double* e0;
+    float* d[8];
+    double* es;
+    float* w[5];
+    float* bc[3];
+    float* bf[3];
+    double ggas, rho_floor, eps_floor;
+    unsigned int* flag;
+};
+
+// FINAL: the state is U^n (after stage 3); otherwise U^n + d
+template <int MODEL, bool FINAL>
+__global__ void __launch_bounds__(256) k_utop_mx(Box b, UtopMx a) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total || (b.skip && *b.skip)) return;
+    const int j = (int)(t % n0);
+    const int k = (int)((t / n0) % n1);
+    const int l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const bool interior = j >= 1 && k >= 1 && l >= 1;
+    auto U = [&](int q, int at) -> double {
+        const double v = df_val(a.uh[q][at], a.ul[q][at]);
+        return FINAL ? v : v + (double)a.d[q][at];
+    };
+    const int off[3] = {1, b.SX, b.SX * b.SY};
+    double bcv[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double face = U(IBX + q, i);
+        a.bf[q][i] = (float)face;
+        if (interior) {
+            bcv[q] = 0.5 * (face + U(IBX + q, i - off[q]));
+            a.bc[q][i] = (float)bcv[q];
+        } else {
+            bcv[q] = a.bc[q][i];
+        }
+    }
+    const double bsq = (bcv[0] * bcv[0] + bcv[1] * bcv[1]) + bcv[2] * bcv[2];
+    const double rho = U(IRHO, i);
+    const double vx = U(IVX, i) / rho, vy = U(IVY, i) / rho, vz = U(IVZ, i) / rho;
+    const double vsq = (vx * vx + vy * vy) + vz * vz;
+    const double E = FINAL ? a.e0[i] : a.es[i];
+    double e = (E - 0.5 * bsq) / rho - 0.5 * vsq;
+    double rn = rho;
+    bool changed = false;
+    if (interior) {
+        if (MODEL == 1) {
+            if (e < 0.0) { e = 0.0; changed = true; }
+        } else if (MODEL == 2 || MODEL == 3) {
+            if (rn < a.rho_floor) { rn = a.rho_floor; changed = true; }
+            if (e < a.eps_floor) { e = a.eps_floor; changed = true; }
+        }
+    }
+    if (changed) {  // FROMRVETOU after CUSTOM_CHECKRHO: re-derive U from the floored prims
+        const double un[4] = {rn, vx * rn, vy * rn, vz * rn};
+        const double En = rn * (e + 0.5 * vsq) + 0.5 * bsq;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (FINAL) {
+                float hi, lo;
+                df_split(un[q], hi, lo);
+                a.uh[q][i] = hi;
+                a.ul[q][i] = lo;
+            } else {
+                a.d[q][i] = (float)(un[q] - df_val(a.uh[q][i], a.ul[q][i]));
+            }
+        }
+        if (FINAL) a.e0[i] = En;
+        else a.es[i] = En;
+    }
+    const double p = (rn * e) * (a.ggas - 1.0);
+    a.w[0][i] = (float)rn;
+    a.w[1][i] = (float)vx;
+    a.w[2][i] = (float)vy;
+    a.w[3][i] = (float)vz;
+    if (interior) {
+        a.w[4][i] = (float)p;
+        if (!(isfinite(p) && isfinite(vsq) && isfinite(rn))) atomicOr(a.flag, 1u);
+    }
+}
+
+// initial_update from the uploaded FP64 model (AoS staging): CUSTOM_CHECKRHO,
+// bcell, P_to_U into hi/lo + FP64 energy, FP32 prims
+template <int MODEL>
+__global__ void __launch_bounds__(256) k_initial_mx(Box b, UtopMx a, const double* __restrict__ prim,
+                                                    const double* __restrict__ eps) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int j = (int)(t % n0);
+    const int k = (int)((t / n0) % n1);
+    const int l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const bool interior = j >= 1 && k >= 1 && l >= 1;
+    const int off[3] = {1, b.SX, b.SX * b.SY};
+    double bcv[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double face = prim[8LL * i + IBX + q];
+        float hi, lo;
+        df_split(face, hi, lo);
+        a.uh[IBX + q][i] = hi;
+        a.ul[IBX + q][i] = lo;
+        a.bf[q][i] = hi;
+        if (interior) {
+            bcv[q] = 0.5 * (face + prim[8LL * (i - off[q]) + IBX + q]);
+            a.bc[q][i] = (float)bcv[q];
+        } else {
+            bcv[q] = 0.0;
+        }
+    }
+    double rho = prim[8LL * i + IRHO];
+    const double vx = prim[8LL * i + IVX], vy = prim[8LL * i + IVY], vz = prim[8LL * i + IVZ];
+    double e = eps[i];
+    if (interior) {
+        if (MODEL == 1) e = fmax(e, 0.0);
+        else if (MODEL == 2 || MODEL == 3) {
+            if (rho < a.rho_floor) rho = a.rho_floor;
+            if (e < a.eps_floor) e = a.eps_floor;
+        }
+    }
+    const double bsq = (bcv[0] * bcv[0] + bcv[1] * bcv[1]) + bcv[2] * bcv[2];
+    const double vsq = (vx * vx + vy * vy) + vz * vz;
+    const double un[4] = {rho, vx * rho, vy * rho, vz * rho};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float hi, lo;
+        df_split(un[q], hi, lo);
+        a.uh[q][i] = hi;
+        a.ul[q][i] = lo;
+    }
+    a.e0[i] = rho * (e + 0.5 * vsq) + 0.5 * bsq;
+    a.w[0][i] = (float)rho;
+    a.w[1][i] = (float)vx;
+    a.w[2][i] = (float)vy;
+    a.w[3][i] = (float)vz;
+    a.w[4][i] = (float)((rho * e) * (a.ggas - 1.0));
+}
+
+// state -> FP64 AoS in the reference layout
+template <int WHAT>
+__global__ void __launch_bounds__(256) k_export_mx(Box b, UtopMx a, double* __restrict__ out) {
+    const long long n = b.count();
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = (int)t;
+    if (WHAT == 0) {  // prim
+        for (int q = 0; q < 5; ++q) out[8 * t + q] = a.w[q][i];
+        for (int q = 0; q < 3; ++q) out[8 * t + 5 + q] = a.bf[q][i];
+    } else if (WHAT == 1) {  // cons
+        for (int q = 0; q < 8; ++q)
+            out[8 * t + q] = q == ITAU ? a.e0[i] : df_val(a.uh[q][i], a.ul[q][i]);
+    } else if (WHAT == 2) {  // eps = p / rho / (g-1)
+        out[t] = ((double)a.w[4][i] / (double)a.w[0][i]) / (a.ggas - 1.0);
+    } else if (WHAT == 3) {
+        for (int q = 0; q < 3; ++q) out[3 * t + q] = a.bc[q][i];
+    } else {  // face fields as three SoA arrays
+        for (int q = 0; q < 3; ++q) out[q * n + t] = df_val(a.uh[IBX + q][i], a.ul[IBX + q][i]);
+    }
+}
+
+template <int DIR>
+void sweep_mx(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>& pr, float ggas, const MixedBufs& m,
+              int recon) {
+    FaceFluxT<float> out;
+    for (int q = 0; q < 7; ++q) out.f[q] = m.F[DIR][q];
+    const dim3 grid = sweep_grid<DIR>(b);
+    if (recon == 4)
+        run(L, DIR, grid, SW_THREADS, sw_smem<float>(), k_sweep_tile<DIR, 4, float>, b, T, pr, ggas, out);
+    else
+        run(L, DIR, grid, SW_THREADS, sw_smem<float>(), k_sweep_tile<DIR, 1, float>, b, T, pr, ggas, out);
+}
+
+UtopMx utop_args(const MixedBufs& m, const MixedParams& p) {
+    UtopMx a;
+    for (int q = 0; q < 8; ++q) { a.uh[q] = m.uh[q]; a.ul[q] = m.ul[q]; a.d[q] = m.d[q]; }
+    a.e0 = m.e0;
+    a.es = m.es;
+    for (int q = 0; q < 5; ++q) a.w[q] = m.w[q];
+    for (int q = 0; q < 3; ++q) { a.bc[q] = m.bc[q]; a.bf[q] = m.bf[q]; }
+    a.ggas = p.ggas;
+    a.rho_floor = p.rho_floor;
+    a.eps_floor = p.eps_floor;
+    a.flag = m.flag;
+    return a;
+}
+
+void boundary_mx(const Launcher& L, const Box& b, const MixedBufs& m, const MixedParams& p) {
+    BoundArgsT<float> a;
+    for (int q = 0; q < 5; ++q) a.w[q] = m.w[q];
+    for (int q = 0; q < 3; ++q) { a.bc[q] = m.bc[q]; a.bf[q] = m.bf[q]; }
+    a.eps = nullptr;
+    for (int q = 0; q < 6; ++q) a.flag[q] = p.flag[q];
+    a.eps_yout = p.eps_yout;
+    for (int s = 0; s < 6; ++s)
+        for (int q = 0; q < 8; ++q) a.fac[s][q] = p.fac[s][q];
+    a.ggas = p.ggas;
+    const long long n = 6LL * b.SX * b.SY + 6LL * b.SX * b.nz + 6LL * b.ny * b.nz;
+    switch (p.model) {
+        case 2: run(L, 6, g1(n, 256), 256, 0, k_boundary<2, float>, b, a); break;
+        case 3: run(L, 6, g1(n, 256), 256, 0, k_boundary<3, float>, b, a); break;
+        default: run(L, 6, g1(n, 256), 256, 0, k_boundary<0, float>, b, a); break;
+    }
+}
+
+template <int COORD, int MODEL>
+void combine_mx(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p, int stage) {
+    FaceFluxT<float> ff[3];
+    for (int d = 0; d < 3; ++d)
+        for (int q = 0; q < 7; ++q) ff[d].f[q] = m.F[d][q];
+    CombineMx a;
+    for (int q = 0; q < 8; ++q) { a.uh[q] = m.uh[q]; a.ul[q] = m.ul[q]; a.d[q] = m.d[q]; }
+    a.e0 = m.e0;
+    a.es = m.es;
+    for (int q = 0; q < 5; ++q) a.w[q] = m.w[q];
+    for (int q = 0; q < 3; ++q) { a.bc[q] = m.bc[q]; a.ecorn[q] = m.E[q]; }
+    a.dt = m.dt;
+    a.geom_repeat = p.geom_repeat;
+    a.rho_floor = (float)p.rho_floor;
+    a.r_sh = (float)p.r_sh;
+    const dim3 g = g1((long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256);
+    if (stage == 1) run(L, 4, g, 256, 0, k_combine_mx<COORD, MODEL, 1>, b, T, ff[0], ff[1], ff[2], a);
+    else if (stage == 2) run(L, 4, g, 256, 0, k_combine_mx<COORD, MODEL, 2>, b, T, ff[0], ff[1], ff[2], a);
+    else run(L, 4, g, 256, 0, k_combine_mx<COORD, MODEL, 3>, b, T, ff[0], ff[1], ff[2], a);
+}
+
+template <int COORD>
+void combine_model_mx(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p,
+                      int stage) {
+    switch (p.model) {
+        case 0: combine_mx<COORD, 0>(L, b, T, m, p, stage); break;
+        case 1: combine_mx<COORD, 1>(L, b, T, m, p, stage); break;
+        case 2: combine_mx<COORD, 2>(L, b, T, m, p, stage); break;
+        default: combine_mx<COORD, 3>(L, b, T, m, p, stage); break;
+    }
+}
+
+}  // namespace
+
+cudaError_t mixed_attributes() {
+    const void* k[6] = {(const void*)k_sweep_tile<0, 4, float>, (const void*)k_sweep_tile<1, 4, float>,
+                        (const void*)k_sweep_tile<2, 4, float>, (const void*)k_sweep_tile<0, 1, float>,
+                        (const void*)k_sweep_tile<1, 1, float>, (const void*)k_sweep_tile<2, 1, float>};
+    for (const void* f : k) {
+        cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw_smem<float>());
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+void mixed_stage(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p, int stage) {
+    PrimT<float> pr;
+    for (int q = 0; q < 5; ++q) pr.w[q] = m.w[q];
+    for (int q = 0; q < 3; ++q) { pr.bc[q] = m.bc[q]; pr.bf[q] = m.bf[q]; }
+    const float ggas = (float)p.ggas;
+    sweep_mx<0>(L, b, T, pr, ggas, m, p.recon);
+    sweep_mx<1>(L, b, T, pr, ggas, m, p.recon);
+    sweep_mx<2>(L, b, T, pr, ggas, m, p.recon);
+    FaceFluxT<float> ff[3];
+    for (int d = 0; d < 3; ++d)
+        for (int q = 0; q < 7; ++q) ff[d].f[q] = m.F[d][q];
+    EdgeET<float> ee;
+    for (int q = 0; q < 3; ++q) ee.e[q] = m.E[q];
+    run(L, 3, g1((long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256), 256, 0, k_emf<float>, b, pr, ff[0], ff[1],
+        ff[2], ee);
+    switch (p.coord) {
+        case 1: combine_model_mx<1>(L, b, T, m, p, stage); break;
+        case 2: combine_model_mx<2>(L, b, T, m, p, stage); break;
+        default: combine_model_mx<3>(L, b, T, m, p, stage); break;
+    }
+    const UtopMx a = utop_args(m, p);
+    const dim3 g = g1((long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256);
+#define CUMC_MX_UTOP(M)                                                       \
+    if (stage == 3) run(L, 5, g, 256, 0, k_utop_mx<M, true>, b, a);           \
+    else run(L, 5, g, 256, 0, k_utop_mx<M, false>, b, a);
+    switch (p.model) {
+        case 0: CUMC_MX_UTOP(0) break;
+        case 1: CUMC_MX_UTOP(1) break;
+        case 2: CUMC_MX_UTOP(2) break;
+        default: CUMC_MX_UTOP(3) break;
+    }
+#undef CUMC_MX_UTOP
+    boundary_mx(L, b, m, p);
+}
+
+void mixed_initial(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p,
+                   const double* prim_aos, const double* eps_aos) {
+    (void)T;
+    const UtopMx a = utop_args(m, p);
+    const dim3 g = g1((long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256);
+    switch (p.model) {
+        case 0: run(L, -1, g, 256, 0, k_initial_mx<0>, b, a, prim_aos, eps_aos); break;
+        case 1: run(L, -1, g, 256, 0, k_initial_mx<1>, b, a, prim_aos, eps_aos); break;
+        case 2: run(L, -1, g, 256, 0, k_initial_mx<2>, b, a, prim_aos, eps_aos); break;
+        default: run(L, -1, g, 256, 0, k_initial_mx<3>, b, a, prim_aos, eps_aos); break;
+    }
+    boundary_mx(L, b, m, p);
+}
+
+void mixed_finddt(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p,
+                  unsigned long long* dtmin) {
+    PrimT<float> pr;
+    for (int q = 0; q < 5; ++q) pr.w[q] = m.w[q];
+    for (int q = 0; q < 3; ++q) { pr.bc[q] = m.bc[q]; pr.bf[q] = m.bf[q]; }
+    const dim3 g = g1((long long)b.nx * b.ny * b.nz, 256);
+    switch (p.coord) {
+        case 1: run(L, 7, g, 256, 0, k_finddt<1, float>, b, T, pr, p.ggas, p.cfl, dtmin); break;
+        case 2: run(L, 7, g, 256, 0, k_finddt<2, float>, b, T, pr, p.ggas, p.cfl, dtmin); break;
+        default: run(L, 7, g, 256, 0, k_finddt<3, float>, b, T, pr, p.ggas, p.cfl, dtmin); break;
+    }
+}
+
+void mixed_export(const Launcher& L, const Box& b, const MixedBufs& m, const MixedParams& p, int what, double* aos) {
+    const UtopMx a = utop_args(m, p);
+    const dim3 g = g1(b.count(), 256);
+    switch (what) {
+        case 0: run(L, -1, g, 256, 0, k_export_mx<0>, b, a, aos); break;
+        case 1: run(L, -1, g, 256, 0, k_export_mx<1>, b, a, aos); break;
+        case 2: run(L, -1, g, 256, 0, k_export_mx<2>, b, a, aos); break;
+        case 3: run(L, -1, g, 256, 0, k_export_mx<3>, b, a, aos); break;
+        default: run(L, -1, g, 256, 0, k_export_mx<4>, b, a, aos); break;
+    }
+}
+
+}  // namespace cumc
