@@ -8,6 +8,7 @@
 #include "cumc_kernels.cuh"
 #include "cumc_sweep.cuh"
 #include "cumc_mixed.h"
+#include "cumc_walk.cuh"
 
 #include <cmath>
 #include <cstdarg>
@@ -68,7 +69,9 @@ struct cumc_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     double graph_t_end = 0.0;
     long long graph_launches_per_step = 0;
-    bool sweep_simple = false;  // CUMC_SWEEP=simple selects the one-thread-per-face sweep
+    // sweep kernels (CUMC_SWEEP): 0 "walk" (default: per-face x, column walker
+    // y/z), 1 "simple" (per-face in all directions), 2 "tile" (shared-memory tiles)
+    int sweep_mode = 0;
     bool mixed = false;         // CUMC_MIXED: state and kernels of cumc_mixed.cu
     MixedBufs mb{};
     MixedParams mp{};
@@ -195,7 +198,19 @@ template <int DIR>
 void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
     FaceFlux out;
     for (int q = 0; q < 7; ++q) out.f[q] = c->F[DIR][q];
-    if (c->sweep_simple) {  // one thread per face, no sharing between faces
+    if (DIR > 0 && c->sweep_mode == 0) {  // column walker along y or z
+        constexpr int D = DIR > 0 ? DIR : 1;
+        int nseg;
+        const int nd = D == 1 ? b.ny : b.nz;
+        const int seg = walk_segment(nd + 1, 64, &nseg);
+        const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
+        if (c->recon == CUMC_PPMC)
+            launch_grid(c, CUMC_K_SWEEP_X + DIR, grid, WK_THREADS, 0, k_sweep_walk<D, 4, double>, b, c->tabs, pr, c->ggas, out, seg);
+        else
+            launch_grid(c, CUMC_K_SWEEP_X + DIR, grid, WK_THREADS, 0, k_sweep_walk<D, 1, double>, b, c->tabs, pr, c->ggas, out, seg);
+        return;
+    }
+    if (c->sweep_mode != 2) {  // one thread per face
         const long long n = (long long)((DIR == 0 ? b.nx : b.nx + 1) + 1) * ((DIR == 1 ? b.ny : b.ny + 1) + 1) *
                             ((DIR == 2 ? b.nz : b.nz + 1) + 1);
         if (c->recon == CUMC_PPMC)
@@ -494,7 +509,7 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     if ((e = cudaGetDevice(&c->device)) != cudaSuccess) { cuda_fail(c, e, "cudaGetDevice"); return fail_init(CUMC_ERR_CUDA); }
     {
         const char* sw = getenv("CUMC_SWEEP");
-        c->sweep_simple = sw && std::strcmp(sw, "simple") == 0;
+        c->sweep_mode = !sw ? 0 : std::strcmp(sw, "simple") == 0 ? 1 : std::strcmp(sw, "tile") == 0 ? 2 : 0;
     }
     if ((rc = sweep_attributes(c)) != CUMC_OK) return fail_init(rc);
     c->mixed = cfg->precision == CUMC_MIXED;
@@ -580,10 +595,10 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
         MixedBufs& m = c->mb;
         for (int q = 0; q < 8; ++q) {
             if (q == ITAU) continue;
-            if ((rc = ffield(&m.uh[q])) != CUMC_OK || (rc = ffield(&m.ul[q])) != CUMC_OK ||
-                (rc = ffield(&m.d[q])) != CUMC_OK)
-                return fail_init(rc);
+            if ((rc = ffield(&m.uh[q])) != CUMC_OK || (rc = ffield(&m.ul[q])) != CUMC_OK) return fail_init(rc);
+            if (q < ITAU && (rc = ffield(&m.d[q])) != CUMC_OK) return fail_init(rc);
         }
+        for (int q = 0; q < 3; ++q) if ((rc = field(&m.db[q])) != CUMC_OK) return fail_init(rc);
         if ((rc = field(&m.e0)) != CUMC_OK || (rc = field(&m.es)) != CUMC_OK) return fail_init(rc);
         for (int q = 0; q < 5; ++q) if ((rc = ffield(&m.w[q])) != CUMC_OK) return fail_init(rc);
         for (int q = 0; q < 3; ++q)
@@ -826,9 +841,7 @@ int cumc_advance(cumc_ctx* c, int nsteps, double t_end, double* t_inout, int* st
     if (nsteps < 0 || !t_inout) return c->fail(CUMC_ERR_ARG, "nsteps must be >= 0 and t_inout non-null");
     launch(c, -1, 1, 1, k_set_scalar, c->scal + 1, *t_inout);
     CUMC_CHECK(cudaMemsetAsync(c->ints, 0, 2 * sizeof(int), c->stream));
-    if (c->prof_on) {
-        for (int s = 0; s < nsteps; ++s) loop_step(c, t_end);
-    } else if (nsteps > 0) {
+    if (nsteps > 0 && !c->prof_on) {
         if (!c->graph_exec || c->graph_t_end != t_end) {
             if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
             cudaGraph_t g;
@@ -844,9 +857,29 @@ int cumc_advance(cumc_ctx* c, int nsteps, double t_end, double* t_inout, int* st
             c->graph_t_end = t_end;
             c->graph_launches_per_step = per_step;
         }
-        for (int s = 0; s < nsteps; ++s) {
-            CUMC_CHECK(cudaGraphLaunch(c->graph_exec, c->stream));
-            c->launches += c->graph_launches_per_step;
+    }
+    // Steps are issued in chunks; between chunks the host reads t back and
+    // stops once it has reached t_end (steps issued after that are no-ops on
+    // the device through the done flag, so at most one chunk is wasted).
+    constexpr int kChunk = 64;
+    int issued = 0;
+    while (issued < nsteps) {
+        const int m = nsteps - issued < kChunk ? nsteps - issued : kChunk;
+        for (int s = 0; s < m; ++s) {
+            if (c->prof_on) {
+                loop_step(c, t_end);
+            } else {
+                CUMC_CHECK(cudaGraphLaunch(c->graph_exec, c->stream));
+                c->launches += c->graph_launches_per_step;
+            }
+        }
+        issued += m;
+        if (issued < nsteps) {
+            CUMC_CHECK(cudaMemcpyAsync(c->host_pinned + 3, c->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            CUMC_CHECK(cudaStreamSynchronize(c->stream));
+            double t_now;
+            std::memcpy(&t_now, c->host_pinned + 3, sizeof(double));
+            if (!(t_now < t_end)) break;
         }
     }
     CUMC_CHECK(cudaMemcpyAsync(c->host_pinned, c->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));

@@ -143,47 +143,52 @@ __device__ __forceinline__ R fluxhll(R yl, R yr, R xl, R xr, R sl, R sr) {
     return ((sr * yl - sl * yr) + (sl * sr) * (xr - xl)) / (sr - sl);
 }
 
-// One side of the face: conserved state (PtoU_MHD_face, solver/ptou_face.f90:34-88)
-// and physical flux (Ptof_MHD, solver/flux.f90:163-262). w is in natural
-// order (rho, vx, vy, vz, p, bx, by, bz); u and f receive the 8 components.
+// One side of the face (PtoU_MHD_face, solver/ptou_face.f90:34-88, and
+// Ptof_MHD, solver/flux.f90:163-262), kept as the few scalars every conserved
+// and flux component is formed from, so that the HLL combination below can
+// form one component at a time (each with the reference's expression tree)
+// instead of holding four 8-vectors live.
 template <int DIR, typename R>
-__device__ __forceinline__ void side_state(const R w[8], R ggas, R u[8], R f[8]) {
-    constexpr int ivn = IVX + DIR, ivt1 = IVX + (DIR + 1) % 3, ivt2 = IVX + (DIR + 2) % 3;
-    constexpr int ibn = IBX + DIR, ibt1 = IBX + (DIR + 1) % 3, ibt2 = IBX + (DIR + 2) % 3;
-    const R rho = w[IRHO], vx = w[IVX], vy = w[IVY], vz = w[IVZ], p = w[ITAU];
-    const R bx = w[IBX], by = w[IBY], bz = w[IBZ];
-    const R e = (p / rho) / (ggas - R(1));  // EOS_EPSILON (model/riemann/src/eos.f90:194)
-    const R vsquare = (vx * vx + vy * vy) + vz * vz;
-    const R bsquare = (bx * bx + by * by) + bz * bz;
-    u[IRHO] = rho;
-    u[IVX] = vx * rho;
-    u[IVY] = vy * rho;
-    u[IVZ] = vz * rho;
-    u[ITAU] = rho * (e + R(0.5) * vsquare) + R(0.5) * bsquare;
-    u[IBX] = bx;
-    u[IBY] = by;
-    u[IBZ] = bz;
-    const R vdotb = (bx * vx + by * vy) + bz * vz;
-    const R vn = w[ivn], bn = w[ibn];
-#pragma unroll
-    for (int i = 0; i < 5; ++i) f[i] = u[i] * vn;
-    f[ivn] = ((f[ivn] + p) + R(0.5) * bsquare) - bn * bn;
-    f[ivt1] = f[ivt1] - bn * w[ibt1];
-    f[ivt2] = f[ivt2] - bn * w[ibt2];
-    f[ITAU] = (f[ITAU] + (p + R(0.5) * bsquare) * vn) - bn * vdotb;
-    f[ibn] = R(0);
-    f[ibt1] = vn * w[ibt1] - w[ivt1] * bn;
-    f[ibt2] = vn * w[ibt2] - w[ivt2] * bn;
-}
+struct FaceSide {
+    static constexpr int t1 = (DIR + 1) % 3, t2 = (DIR + 2) % 3;
+    R rho, v[3], p, b[3], E, hb2, vdotb;
+    __device__ __forceinline__ FaceSide(const R w[8], R ggas) {
+        rho = w[IRHO];
+        v[0] = w[IVX]; v[1] = w[IVY]; v[2] = w[IVZ];
+        p = w[ITAU];
+        b[0] = w[IBX]; b[1] = w[IBY]; b[2] = w[IBZ];
+        const R e = (p / rho) / (ggas - R(1));  // EOS_EPSILON (model/riemann/src/eos.f90:194)
+        const R vsquare = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
+        const R bsquare = (b[0] * b[0] + b[1] * b[1]) + b[2] * b[2];
+        E = rho * (e + R(0.5) * vsquare) + R(0.5) * bsquare;
+        hb2 = R(0.5) * bsquare;
+        vdotb = (b[0] * v[0] + b[1] * v[1]) + b[2] * v[2];
+    }
+    // conserved component q
+    __device__ __forceinline__ R u(int q) const {
+        return q == IRHO ? rho : q <= IVZ ? v[q - IVX] * rho : q == ITAU ? E : b[q - IBX];
+    }
+    // flux component q along DIR (q != IBX+DIR, whose flux is 0)
+    __device__ __forceinline__ R f(int q) const {
+        const R vn = v[DIR], bn = b[DIR];
+        if (q == IRHO) return rho * vn;
+        if (q == IVX + DIR) return ((v[DIR] * rho * vn + p) + hb2) - bn * bn;
+        if (q == IVX + t1) return v[t1] * rho * vn - bn * b[t1];
+        if (q == IVX + t2) return v[t2] * rho * vn - bn * b[t2];
+        if (q == ITAU) return (E * vn + (p + hb2) * vn) - bn * vdotb;
+        if (q == IBX + t1) return vn * b[t1] - v[t1] * bn;
+        return vn * b[t2] - v[t2] * bn;  // IBX + t2
+    }
+};
 
-// HLL flux at a face from the left and right primitive states.
+// HLL flux at a face from the left and right primitive states (8 each,
+// natural order). out receives the 7 stored components: rho, rho v, E and
+// the two tangential fields in natural (x, y, z) order.
 template <int DIR, typename R>
-__device__ __forceinline__ void hll_flux(const R wl[8], const R wr[8], R ggas, R flux[8]) {
+__device__ __forceinline__ void hll_flux7(const R wl[8], const R wr[8], R ggas, R out[7]) {
     constexpr int ivn = IVX + DIR;
     constexpr int ibn = IBX + DIR, ibt1 = IBX + (DIR + 1) % 3, ibt2 = IBX + (DIR + 2) % 3;
-    R ul[8], ur[8], fl[8], fr[8];
-    side_state<DIR>(wl, ggas, ul, fl);
-    side_state<DIR>(wr, ggas, ur, fr);
+    const FaceSide<DIR, R> L(wl, ggas), Rs(wr, ggas);
     // EOS_SOUNDSPEED (model/riemann/src/eos.f90:168)
     const R csL = sqrt((ggas * wl[ITAU]) / wl[IRHO]);
     const R csR = sqrt((ggas * wr[ITAU]) / wr[IRHO]);
@@ -194,15 +199,18 @@ __device__ __forceinline__ void hll_flux(const R wl[8], const R wr[8], R ggas, R
     const R cbar = roe_avg(cfsL, cfsR, sqL, sqR);
     const R sL = fmin(wl[ivn] - cfsL, ubar - cbar);
     const R sR = fmax(wr[ivn] + cfsR, ubar + cbar);
+    constexpr int bt_a = DIR == 0 ? IBY : IBX;  // stored tangential components
+    constexpr int bt_b = DIR == 2 ? IBY : IBZ;
+    const int comp[7] = {IRHO, IVX, IVY, IVZ, ITAU, bt_a, bt_b};
     if (sL >= R(0)) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) flux[i] = fl[i];
+        for (int c = 0; c < 7; ++c) out[c] = L.f(comp[c]);
     } else if (sL <= R(0) && sR >= R(0)) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) flux[i] = fluxhll(fl[i], fr[i], ul[i], ur[i], sL, sR);
+        for (int c = 0; c < 7; ++c) out[c] = fluxhll(L.f(comp[c]), Rs.f(comp[c]), L.u(comp[c]), Rs.u(comp[c]), sL, sR);
     } else {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) flux[i] = fr[i];
+        for (int c = 0; c < 7; ++c) out[c] = Rs.f(comp[c]);
     }
 }
 

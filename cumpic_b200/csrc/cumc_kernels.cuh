@@ -39,8 +39,8 @@ struct Cons {
 // cells (INTERPOLATE, solver/spatial.f90:131-154) and solves the Riemann
 // problem (HLL_SOLVER).
 // ----------------------------------------------------------------------------
-template <int DIR, int RECON>
-__global__ void __launch_bounds__(128) k_sweep(Box b, Tabs T, Prim pr, double ggas, FaceFlux out) {
+template <int DIR, int RECON, typename R = double>
+__global__ void __launch_bounds__(128) k_sweep(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out) {
     const int n0 = (DIR == 0 ? b.nx : b.nx + 1) + 1;
     const int n1 = (DIR == 1 ? b.ny : b.ny + 1) + 1;
     const int n2 = (DIR == 2 ? b.nz : b.nz + 1) + 1;
@@ -58,50 +58,48 @@ __global__ void __launch_bounds__(128) k_sweep(Box b, Tabs T, Prim pr, double gg
     // variables reconstructed along DIR, in natural order
     constexpr int bt_a = DIR == 0 ? 1 : 0;  // first transverse field component
     constexpr int bt_b = DIR == 2 ? 1 : 2;  // second transverse field component
-    const double* src[7] = {pr.w[0], pr.w[1], pr.w[2], pr.w[3], pr.w[4], pr.bc[bt_a], pr.bc[bt_b]};
+    const R* src[7] = {pr.w[0], pr.w[1], pr.w[2], pr.w[3], pr.w[4], pr.bc[bt_a], pr.bc[bt_b]};
     const int slot[7] = {IRHO, IVX, IVY, IVZ, ITAU, IBX + bt_a, IBX + bt_b};
 
-    double wl[8], wr[8];
+    R wl[8], wr[8];
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
-        const double* q = src[v] + base;
-        double w[6];
+        const R* q = src[v] + base;
+        R w[6];
 #pragma unroll
         for (int m = 0; m < 6; ++m) w[m] = q[(m - 2) * s];  // cells c-2 .. c+3
-        double left, right;
+        R left, right;
         if (RECON == 4) {
-            const double d1 = ppm_slope(w[0], w[1], w[2], A.s0[c - 1], A.s1[c - 1]);
-            const double d2 = ppm_slope(w[1], w[2], w[3], A.s0[c], A.s1[c]);
-            const double d3 = ppm_slope(w[2], w[3], w[4], A.s0[c + 1], A.s1[c + 1]);
-            const double d4 = ppm_slope(w[3], w[4], w[5], A.s0[c + 2], A.s1[c + 2]);
-            const double f0 = ppm_face(w[1], w[2], d1, d2, A.a0[c - 1], A.a1[c - 1], A.a2[c - 1], A.a3[c - 1]);
-            const double f1 = ppm_face(w[2], w[3], d2, d3, A.a0[c], A.a1[c], A.a2[c], A.a3[c]);
-            const double f2 = ppm_face(w[3], w[4], d3, d4, A.a0[c + 1], A.a1[c + 1], A.a2[c + 1], A.a3[c + 1]);
-            double vm, vp;
+            const R d1 = ppm_slope(w[0], w[1], w[2], (R)A.s0[c - 1], (R)A.s1[c - 1]);
+            const R d2 = ppm_slope(w[1], w[2], w[3], (R)A.s0[c], (R)A.s1[c]);
+            const R d3 = ppm_slope(w[2], w[3], w[4], (R)A.s0[c + 1], (R)A.s1[c + 1]);
+            const R d4 = ppm_slope(w[3], w[4], w[5], (R)A.s0[c + 2], (R)A.s1[c + 2]);
+            const R f0 = ppm_face(w[1], w[2], d1, d2, (R)A.a0[c - 1], (R)A.a1[c - 1], (R)A.a2[c - 1], (R)A.a3[c - 1]);
+            const R f1 = ppm_face(w[2], w[3], d2, d3, (R)A.a0[c], (R)A.a1[c], (R)A.a2[c], (R)A.a3[c]);
+            const R f2 = ppm_face(w[3], w[4], d3, d4, (R)A.a0[c + 1], (R)A.a1[c + 1], (R)A.a2[c + 1], (R)A.a3[c + 1]);
+            R vm, vp;
             ppm_fix(w[2], f0, f1, vm, vp);
             left = vp;   // primL at face c = vp_out of cell c
             ppm_fix(w[3], f1, f2, vm, vp);
             right = vm;  // primR at face c = vm_out of cell c+1
         } else {
-            const double sl = tvd_slope(w[1], w[2], w[3], A.tcf[c], A.tcb[c]);
-            const double sr = tvd_slope(w[2], w[3], w[4], A.tcf[c + 1], A.tcb[c + 1]);
-            left = w[2] + 0.5 * sl;
-            right = w[3] - 0.5 * sr;
+            const R sl = tvd_slope(w[1], w[2], w[3], (R)A.tcf[c], (R)A.tcb[c]);
+            const R sr = tvd_slope(w[2], w[3], w[4], (R)A.tcf[c + 1], (R)A.tcb[c + 1]);
+            left = w[2] + R(0.5) * sl;
+            right = w[3] - R(0.5) * sr;
         }
         wl[slot[v]] = left;
         wr[slot[v]] = right;
     }
     // normal field: the shared face value (solver/spatial.f90:148-149)
-    const double bn = pr.bf[DIR][base];
+    const R bn = pr.bf[DIR][base];
     wl[IBX + DIR] = bn;
     wr[IBX + DIR] = bn;
 
-    double fx[8];
-    hll_flux<DIR>(wl, wr, ggas, fx);
+    R fx[7];
+    hll_flux7<DIR>(wl, wr, ggas, fx);
 #pragma unroll
-    for (int i = 0; i < 5; ++i) out.f[i][base] = fx[i];
-    out.f[5][base] = fx[IBX + bt_a];
-    out.f[6][base] = fx[IBX + bt_b];
+    for (int i = 0; i < 7; ++i) out.f[i][base] = fx[i];
 }
 
 // ----------------------------------------------------------------------------

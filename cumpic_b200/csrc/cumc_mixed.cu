@@ -19,6 +19,7 @@
 // u3 = 1/3 u0 + 2/3 u2 + 2/3 dt L3 in exact arithmetic.
 #include "cumc_mixed.h"
 #include "cumc_sweep.cuh"
+#include "cumc_walk.cuh"
 
 namespace cumc {
 namespace {
@@ -64,6 +65,7 @@ struct CombineMx {
     float* ul[8];
     double* e0;
     float* d[8];
+    double* db[3];
     double* es;
     const float* w[5];
     const float* bc[3];
@@ -132,23 +134,41 @@ __global__ void __launch_bounds__(256) k_combine_mx(Box b, Tabs T, FaceFluxT<flo
             L[ITAU] -= factor * rho * (vx * x + vz * z) * inv;
         }
     }
+    // CT curl of the FP32 edge EMFs, formed in FP64 (solver/mhd.f90:137-148)
+    double LB[3];
     {
         CTf g;
         geom_ct<COORD>(T, j, k, l, g);
         const float* Ex = a.ecorn[0];
         const float* Ey = a.ecorn[1];
         const float* Ez = a.ecorn[2];
-        L[IBX] = -((Ez[i] * (float)g.bx_ez_p - Ez[i - sk] * (float)g.bx_ez_m) * (float)(1.0 / g.bx_ez_c) -
-                   (Ey[i] * (float)g.bx_ey_p - Ey[i - sl] * (float)g.bx_ey_m) * (float)(1.0 / g.bx_ey_c));
-        L[IBY] = -((Ex[i] * (float)g.by_ex_p - Ex[i - sl] * (float)g.by_ex_m) * (float)(1.0 / g.by_ex_c) -
-                   (Ez[i] * (float)g.by_ez_p - Ez[i - sj] * (float)g.by_ez_m) * (float)(1.0 / g.by_ez_c));
-        L[IBZ] = -((Ey[i] * (float)g.bz_ey_p - Ey[i - sj] * (float)g.bz_ey_m) * (float)(1.0 / g.bz_ey_c) -
-                   (Ex[i] * (float)g.bz_ex_p - Ex[i - sk] * (float)g.bz_ex_m) * (float)(1.0 / g.bz_ex_c));
+        auto e = [](const float* E, int at) { return (double)E[at]; };
+        LB[0] = -((e(Ez, i) * g.bx_ez_p - e(Ez, i - sk) * g.bx_ez_m) / g.bx_ez_c -
+                  (e(Ey, i) * g.bx_ey_p - e(Ey, i - sl) * g.bx_ey_m) / g.bx_ey_c);
+        LB[1] = -((e(Ex, i) * g.by_ex_p - e(Ex, i - sl) * g.by_ex_m) / g.by_ex_c -
+                  (e(Ez, i) * g.by_ez_p - e(Ez, i - sj) * g.by_ez_m) / g.by_ez_c);
+        LB[2] = -((e(Ey, i) * g.bz_ey_p - e(Ey, i - sj) * g.bz_ey_m) / g.bz_ey_c -
+                  (e(Ex, i) * g.bz_ex_p - e(Ex, i - sk) * g.bz_ex_m) / g.bz_ex_c);
     }
     const double dt = *a.dt;
     const float dtf = (float)dt;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < 3; ++q) {
+        double* db = a.db[q];
+        if (STAGE == 1) {
+            db[i] = dt * LB[q];
+        } else if (STAGE == 2) {
+            db[i] = 0.25 * (db[i] + dt * LB[q]);
+        } else {
+            const double v = df_val(a.uh[IBX + q][i], a.ul[IBX + q][i]) + (2.0 / 3.0) * (db[i] + dt * LB[q]);
+            float hi, lo;
+            df_split(v, hi, lo);
+            a.uh[IBX + q][i] = hi;
+            a.ul[IBX + q][i] = lo;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
         if (q == ITAU) continue;
         if (STAGE == 1) {
             a.d[q][i] = dtf * L[q];
@@ -178,6 +198,7 @@ struct UtopMx {
     float* ul[8];
     double* e0;
     float* d[8];
+    double* db[3];
     double* es;
     float* w[5];
     float* bc[3];
@@ -200,7 +221,8 @@ __global__ void __launch_bounds__(256) k_utop_mx(Box b, UtopMx a) {
     const bool interior = j >= 1 && k >= 1 && l >= 1;
     auto U = [&](int q, int at) -> double {
         const double v = df_val(a.uh[q][at], a.ul[q][at]);
-        return FINAL ? v : v + (double)a.d[q][at];
+        if (FINAL) return v;
+        return v + (q >= IBX ? a.db[q - IBX][at] : (double)a.d[q][at]);
     };
     const int off[3] = {1, b.SX, b.SX * b.SY};
     double bcv[3];
@@ -315,7 +337,9 @@ __global__ void __launch_bounds__(256) k_initial_mx(Box b, UtopMx a, const doubl
     a.w[1][i] = (float)vx;
     a.w[2][i] = (float)vy;
     a.w[3][i] = (float)vz;
-    a.w[4][i] = (float)((rho * e) * (a.ggas - 1.0));
+    const double p = (rho * e) * (a.ggas - 1.0);
+    a.w[4][i] = (float)p;
+    if (interior && !(isfinite(p) && isfinite(vsq) && isfinite(rho))) atomicOr(a.flag, 1u);
 }
 
 // state -> FP64 AoS in the reference layout
@@ -345,16 +369,24 @@ void sweep_mx(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>
               int recon) {
     FaceFluxT<float> out;
     for (int q = 0; q < 7; ++q) out.f[q] = m.F[DIR][q];
-    const dim3 grid = sweep_grid<DIR>(b);
-    if (recon == 4)
-        run(L, DIR, grid, SW_THREADS, sw_smem<float>(), k_sweep_tile<DIR, 4, float>, b, T, pr, ggas, out);
-    else
-        run(L, DIR, grid, SW_THREADS, sw_smem<float>(), k_sweep_tile<DIR, 1, float>, b, T, pr, ggas, out);
+    if (DIR > 0) {  // column walker along y or z
+        constexpr int D = DIR > 0 ? DIR : 1;
+        int nseg;
+        const int seg = walk_segment(WalkGeom<D>::nd(b) + 1, 64, &nseg);
+        const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
+        if (recon == 4) run(L, DIR, grid, WK_THREADS, 0, k_sweep_walk<D, 4, float>, b, T, pr, ggas, out, seg);
+        else run(L, DIR, grid, WK_THREADS, 0, k_sweep_walk<D, 1, float>, b, T, pr, ggas, out, seg);
+        return;
+    }
+    const long long n = (long long)(b.nx + 1) * (b.ny + 2) * (b.nz + 2);
+    if (recon == 4) run(L, DIR, g1(n, 128), 128, 0, k_sweep<0, 4, float>, b, T, pr, ggas, out);
+    else run(L, DIR, g1(n, 128), 128, 0, k_sweep<0, 1, float>, b, T, pr, ggas, out);
 }
 
 UtopMx utop_args(const MixedBufs& m, const MixedParams& p) {
     UtopMx a;
     for (int q = 0; q < 8; ++q) { a.uh[q] = m.uh[q]; a.ul[q] = m.ul[q]; a.d[q] = m.d[q]; }
+    for (int q = 0; q < 3; ++q) a.db[q] = m.db[q];
     a.e0 = m.e0;
     a.es = m.es;
     for (int q = 0; q < 5; ++q) a.w[q] = m.w[q];
@@ -391,6 +423,7 @@ void combine_mx(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs&
         for (int q = 0; q < 7; ++q) ff[d].f[q] = m.F[d][q];
     CombineMx a;
     for (int q = 0; q < 8; ++q) { a.uh[q] = m.uh[q]; a.ul[q] = m.ul[q]; a.d[q] = m.d[q]; }
+    for (int q = 0; q < 3; ++q) a.db[q] = m.db[q];
     a.e0 = m.e0;
     a.es = m.es;
     for (int q = 0; q < 5; ++q) a.w[q] = m.w[q];

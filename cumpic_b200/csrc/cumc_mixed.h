@@ -2,7 +2,9 @@
 //
 // State of the mixed form, per cell:
 //   U^n  : rho, rho v, B as hi/lo FP32 pairs (compensated), total energy FP64
-//   d_s  : stage increment U_s - U^n as FP32, stage energy FP64
+//   d_s  : stage increment U_s - U^n as FP32 for rho, rho v; FP64 for B (the
+//          CT curl of the FP32 EMFs is formed in FP64 so that the face-field
+//          update keeps div B at round-off); stage energy FP64
 //   prims: rho, v, p, bcell and the current face field as FP32 (with ghosts)
 // Reconstruction, HLL and EMFs run in FP32; the pressure recovery
 // E - rho v^2/2 - B^2/2 and the energy combine run in FP64.
@@ -17,7 +19,9 @@ struct MixedBufs {
     float* uh[8];   // U^n high parts (index 4 unused: energy is e0)
     float* ul[8];   // U^n low parts
     double* e0;     // U^n total energy
-    float* d[8];    // stage increment (index 4 unused)
+    float* d[8];    // stage increment of rho, rho v (indices 0-3; 4-7 unused)
+    double* db[3];  // stage increment of the face fields (FP64: keeps the CT
+                    // update divergence-free to round-off)
     double* es;     // stage total energy
     float* w[5];    // rho, vx, vy, vz, p
     float* bc[3];   // bcell

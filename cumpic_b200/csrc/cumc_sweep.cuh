@@ -160,12 +160,10 @@ __global__ void __launch_bounds__(SW_THREADS, 2) k_sweep_tile(Box b, Tabs T, Pri
     const R bn = pr.bf[DIR][gi];
     wl[IBX + DIR] = bn;
     wr[IBX + DIR] = bn;
-    R fx[8];
-    hll_flux<DIR>(wl, wr, ggas, fx);
+    R fx[7];
+    hll_flux7<DIR>(wl, wr, ggas, fx);
 #pragma unroll
-    for (int i = 0; i < 5; ++i) out.f[i][gi] = fx[i];
-    out.f[5][gi] = fx[IBX + bt_a];
-    out.f[6][gi] = fx[IBX + bt_b];
+    for (int i = 0; i < 7; ++i) out.f[i][gi] = fx[i];
 }
 
 template <int DIR>

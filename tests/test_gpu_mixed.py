@@ -1,0 +1,74 @@
+"""Mixed-precision path (CUMC_MIXED) against the FP64 path.
+
+Bars: relative L1 of the density against the FP64 run <= 1e-5 (the
+north-star's bar for the mixed form) and the normalised max |div B| of the
+compensated face fields at round-off.
+"""
+import numpy as np
+import pytest
+
+from cumpic_b200 import _native as N
+from cumpic_b200 import problems as P
+from compare import rel_l1_interior
+
+pytestmark = pytest.mark.gpu
+
+RHO_L1_TOL = 1.0e-5
+DIVB_TOL = 1.0e-12
+
+
+def _run(problem, precision, steps=None, t_end=None):
+    from cumpic_b200.solver import CUMC3D
+    problem.precision = precision
+    s = CUMC3D(problem)
+    s.upload()
+    s.initial_update()
+    if t_end is not None:
+        s.run(t_end)
+    else:
+        for _ in range(steps):
+            s.step()
+    return s
+
+
+@pytest.mark.parametrize("bscale", [1.0, 10.0])
+def test_orszag_tang_mixed_vs_fp64(bscale):
+    a = _run(P.orszag_tang(32, bscale=bscale), N.FP64, t_end=0.05)
+    b = _run(P.orszag_tang(32, bscale=bscale), N.MIXED, t_end=0.05)
+    rel = rel_l1_interior(b.download(), a.download())
+    assert rel[0] <= RHO_L1_TOL, rel
+    assert max(rel.values()) <= 1e-3, rel
+    _, norm = b.find_divb()
+    assert norm <= DIVB_TOL, norm
+
+
+def test_brio_wu_mixed_vs_fp64():
+    p = P.brio_wu(512, 4, 4)
+    a = _run(P.brio_wu(512, 4, 4), N.FP64, t_end=p.t_end)
+    b = _run(P.brio_wu(512, 4, 4), N.MIXED, t_end=p.t_end)
+    assert b.global_time == pytest.approx(p.t_end)
+    rel = rel_l1_interior(b.download(), a.download())
+    assert rel[0] <= 1e-4, rel  # shocks: FP32 fluxes move discontinuities by round-off
+
+
+def test_torus_mixed_runs_and_tracks_fp64():
+    a = _run(P.torus(48, 32, 16), N.FP64, steps=20)
+    b = _run(P.torus(48, 32, 16), N.MIXED, steps=20)
+    da, db = a.download(), b.download()
+    assert np.all(np.isfinite(db["cons"]))
+    rel = rel_l1_interior(db, da)
+    assert rel[0] <= 1e-4, rel
+
+
+def test_mixed_advance_equals_host_loop():
+    from cumpic_b200.solver import CUMC3D
+    p = P.orszag_tang(16, precision=N.MIXED)
+    x, y = CUMC3D(p), CUMC3D(p)
+    for s in (x, y):
+        s.upload()
+        s.initial_update()
+    for _ in range(5):
+        x.step()
+    y.advance(5)
+    assert x.global_time == y.global_time
+    assert np.array_equal(x.download()["cons"], y.download()["cons"])

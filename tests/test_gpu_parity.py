@@ -171,11 +171,14 @@ def test_call_order_and_config_errors():
     assert e.value.code == N.CUMC_ERR_CONFIG
 
 
-def test_nonfinite_state_is_reported():
-    """A negative density makes the state non-finite; finddt reports it."""
+@pytest.mark.parametrize("precision", [N.FP64, N.MIXED])
+def test_nonfinite_state_is_reported(precision):
+    """A NaN injected into the uploaded model is flagged on the device and
+    reported by the next finddt as CUMC_ERR_NONFINITE (the reference passes
+    NaN and negative pressure through silently, solver/utop.f90:63)."""
     from cumpic_b200.solver import CUMC3D
-    p = P.orszag_tang(8)
-    p.prim[6, 6, 6, 0] = -1.0
+    p = P.orszag_tang(8, precision=precision)
+    p.prim[6, 6, 6, 0] = float("nan")  # eps would be floored by CUSTOM_CHECKRHO's MAX(eps, 0)
     g = CUMC3D(p)
     g.upload()
     g.initial_update()
