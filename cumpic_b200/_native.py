@@ -69,7 +69,7 @@ EXPORTS = [
     "cumc_init", "cumc_free", "cumc_last_error", "cumc_upload_state", "cumc_download_state",
     "cumc_initial_update", "cumc_finddt", "cumc_rungekutta", "cumc_spatial", "cumc_download_lrk",
     "cumc_divb", "cumc_advance", "cumc_get_stream", "cumc_profile", "cumc_profile_read",
-    "cumc_launch_count",
+    "cumc_launch_count", "cumc_cfl_dt_static", "cumc_cfl_dt_static_error",
 ]
 
 
@@ -97,6 +97,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "cumc_profile": (c_int, [c_void_p, c_int]),
         "cumc_profile_read": (c_int, [c_void_p, c_int, POINTER(c_int), dp]),
         "cumc_launch_count": (c_int, [c_void_p, POINTER(c_longlong)]),
+        "cumc_cfl_dt_static": (c_int, [c_int, c_int, c_int] + [c_void_p] * 11 + [c_int, c_void_p, c_void_p,
+                                                                                   c_double, c_double, c_void_p,
+                                                                                   c_void_p]),
+        "cumc_cfl_dt_static_error": (c_char_p, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -1,8 +1,9 @@
 """Build recipe of the CUDA library (sm_100a) and of the CPU oracle.
 
-``build_library()`` compiles cumpic_b200/csrc/cumc_api.cu with nvcc into
-cumpic_b200/libcumc_b200.so. FMA contraction is off so that the FP64 path is
-bit-compatible with the FP64 restatement used as the test oracle.
+``build_library()`` compiles the units in ``UNITS`` (cumpic_b200/csrc) with
+nvcc and links them into cumpic_b200/libcumc_b200.so. FMA contraction is off
+in the FP64 units so that they are bit-compatible with the FP64 restatement
+used as the test oracle.
 """
 from __future__ import annotations
 
@@ -21,7 +22,7 @@ COMMON = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcom
 FP64_FLAGS = ["--fmad=false"]
 # mixed path: FMA and fast FP32 division/square root (FP64 parts stay IEEE).
 MIXED_FLAGS = ["--fmad=true", "-prec-div=false", "-prec-sqrt=false"]
-UNITS = {"cumc_api.cu": FP64_FLAGS, "cumc_mixed.cu": MIXED_FLAGS}
+UNITS = {"cumc_api.cu": FP64_FLAGS, "cumc_mixed.cu": MIXED_FLAGS, "cumc_static.cu": FP64_FLAGS}
 NVCC_FLAGS = COMMON + FP64_FLAGS  # flags of the FP64 unit (kept for tools that print them)
 
 

@@ -175,6 +175,43 @@ int cumc_profile_read(cumc_ctx* ctx, int which, int* launches, double* ms);
 /* Number of kernel launches the library issued since cumc_init. */
 int cumc_launch_count(cumc_ctx* ctx, long long* count);
 
+/* CFL time step over caller-owned device arrays, allocating nothing.
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory when they need a time step, such as a code capturing
+ * its time loop into a CUDA graph (cudaMalloc is not allowed during capture)
+ * or a host program whose device memory is owned by another runtime (an
+ * OpenACC data region, a framework's caching allocator, a fixed pool).
+ *
+ * Inputs are device arrays in the library's layout: one FP64 array per field
+ * over the ghosted box (-2:n+3)^3, x fastest (rho, vx, vy, vz, p, and the
+ * cell-centred field bcx, bcy, bcz), and per-axis cell widths dx, dy, dz with
+ * nx+7 (ny+7, nz+7) entries for indices -3..n+3. Cylindrical and spherical
+ * grids also need the cell-centre radius xc (nx+7 entries) and, spherical,
+ * sin of the polar cell centre sin_yc (ny+7 entries); both may be NULL for
+ * CUMC_CARTESIAN. The result is written to the device double *dt_out; the
+ * work is queued on `stream` (NULL: the default stream) and the call returns
+ * without synchronising.
+ *
+ * Its only scratch, the per-block partial minima, is a fixed device array of
+ * the library (128 KiB per device, held until the process exits), which
+ * limits a call to CUMC_STATIC_MAX_CELLS active cells; larger grids get
+ * CUMC_ERR_LIMIT. The first call on each device looks up that array's device
+ * address (cudaGetSymbolAddress), so make a first call on each device before
+ * any stream capture. Nothing in the array needs to start at zero: each call
+ * writes every entry it later reads. Every call on a device shares the
+ * array, so calls that overlap on the GPU race; order them on one stream or
+ * synchronise between them. cumc_cfl_dt_static_error() describes the last
+ * failure of the calling thread. */
+#define CUMC_STATIC_MAX_CELLS (256 * 256 * 256)
+int cumc_cfl_dt_static(int nx, int ny, int nz,
+                       const double* rho, const double* vx, const double* vy,
+                       const double* vz, const double* p,
+                       const double* bcx, const double* bcy, const double* bcz,
+                       const double* dx, const double* dy, const double* dz,
+                       int coordinate, const double* xc, const double* sin_yc,
+                       double ggas, double cfl, double* dt_out, void* stream);
+const char* cumc_cfl_dt_static_error(void);
+
 #ifdef __cplusplus
 }
 #endif
