@@ -69,8 +69,12 @@ struct cumc_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     double graph_t_end = 0.0;
     long long graph_launches_per_step = 0;
-    // sweep kernels (CUMC_SWEEP): 0 "walk" (default: per-face x, column walker
-    // y/z), 1 "simple" (per-face in all directions), 2 "tile" (shared-memory tiles)
+    // sweep kernels (environment variable CUMC_SWEEP, for A/B timing; all
+    // give the same bits): 0 default (per-face x, shared-memory-window walker
+    // y/z), 1 "simple" (per-face everywhere), 2 "tile" (shared-memory tiles),
+    // 3 "walkx" (register walker everywhere, x staged through shared memory),
+    // 4 "walksm" (shared-memory-window walker everywhere), 5 "walkreg"
+    // (per-face x, register walker y/z)
     int sweep_mode = 0;
     bool mixed = false;         // CUMC_MIXED: state and kernels of cumc_mixed.cu
     MixedBufs mb{};
@@ -198,16 +202,28 @@ template <int DIR>
 void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
     FaceFlux out;
     for (int q = 0; q < 7; ++q) out.f[q] = c->F[DIR][q];
-    if (DIR > 0 && c->sweep_mode == 0) {  // column walker along y or z
-        constexpr int D = DIR > 0 ? DIR : 1;
+    // default: one thread per face along x, the shared-memory-window walker
+    // along y and z (the fastest pairing measured at 256^3)
+    const bool walk = (DIR > 0 && (c->sweep_mode == 0 || c->sweep_mode == 5)) || c->sweep_mode == 3 ||
+                      c->sweep_mode == 4;
+    if (walk) {  // column walker
         int nseg;
-        const int nd = D == 1 ? b.ny : b.nz;
-        const int seg = walk_segment(nd + 1, 64, &nseg);
-        const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
-        if (c->recon == CUMC_PPMC)
-            launch_grid(c, CUMC_K_SWEEP_X + DIR, grid, WK_THREADS, 0, k_sweep_walk<D, 4, double>, b, c->tabs, pr, c->ggas, out, seg);
-        else
-            launch_grid(c, CUMC_K_SWEEP_X + DIR, grid, WK_THREADS, 0, k_sweep_walk<D, 1, double>, b, c->tabs, pr, c->ggas, out, seg);
+        const int seg = walk_segment(WalkGeom<DIR>::nd(b) + 1, 64, &nseg);
+        const dim3 grid((unsigned)((WalkGeom<DIR>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
+        const int cls = CUMC_K_SWEEP_X + DIR;
+        if (c->sweep_mode == 4 || c->sweep_mode == 0) {
+            const size_t sm = walk_smem<double>(DIR);
+            if (c->recon == CUMC_PPMC)
+                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 4, double>, b, c->tabs, pr, c->ggas, out, seg);
+            else
+                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 1, double>, b, c->tabs, pr, c->ggas, out, seg);
+        } else {
+            const size_t sm = DIR == 0 ? xstage_smem<double>() : 0;
+            if (c->recon == CUMC_PPMC)
+                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk<DIR, 4, double>, b, c->tabs, pr, c->ggas, out, seg);
+            else
+                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk<DIR, 1, double>, b, c->tabs, pr, c->ggas, out, seg);
+        }
         return;
     }
     if (c->sweep_mode != 2) {  // one thread per face
@@ -509,7 +525,13 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     if ((e = cudaGetDevice(&c->device)) != cudaSuccess) { cuda_fail(c, e, "cudaGetDevice"); return fail_init(CUMC_ERR_CUDA); }
     {
         const char* sw = getenv("CUMC_SWEEP");
-        c->sweep_mode = !sw ? 0 : std::strcmp(sw, "simple") == 0 ? 1 : std::strcmp(sw, "tile") == 0 ? 2 : 0;
+        c->sweep_mode = !sw                              ? 0
+                        : std::strcmp(sw, "simple") == 0 ? 1
+                        : std::strcmp(sw, "tile") == 0   ? 2
+                        : std::strcmp(sw, "walkx") == 0  ? 3
+                        : std::strcmp(sw, "walksm") == 0 ? 4
+                        : std::strcmp(sw, "walkreg") == 0 ? 5
+                                                          : 0;
     }
     if ((rc = sweep_attributes(c)) != CUMC_OK) return fail_init(rc);
     c->mixed = cfg->precision == CUMC_MIXED;

@@ -186,3 +186,32 @@ def test_nonfinite_state_is_reported(precision):
     with pytest.raises(N.CumcError) as e:
         g.finddt()
     assert e.value.code == N.CUMC_ERR_NONFINITE
+
+
+SWEEP_MODES = ["simple", "tile", "walkx", "walksm", "walkreg"]
+
+
+@pytest.mark.parametrize("mode", SWEEP_MODES)
+def test_sweep_variants_bitwise(mode, monkeypatch):
+    """Every sweep kernel variant (CUMC_SWEEP, read at cumc_init) gives the
+    default variant's bits; ragged sizes exercise partial blocks, segments
+    and x staging chunks."""
+    from cumpic_b200.solver import CUMC3D
+    out = {}
+    for m in (None, mode):
+        if m is None:
+            monkeypatch.delenv("CUMC_SWEEP", raising=False)
+        else:
+            monkeypatch.setenv("CUMC_SWEEP", m)
+        for name, prob in (("ot", P.orszag_tang(37, ny=29, nz=70)), ("tvd", P.orszag_tang(21, recon=N.TVDMM)),
+                           ("torus", P.torus(24, 16, 8))):
+            g = CUMC3D(prob)
+            g.upload()
+            g.initial_update()
+            for _ in range(2):
+                g.rungekutta(g.finddt())
+            out[(m, name)] = g.download()
+            g.close()
+    for name in ("ot", "tvd", "torus"):
+        d = diffs(out[(None, name)], out[(mode, name)])
+        assert all(v == 0.0 for v in d.values()), (name, d)
