@@ -54,6 +54,27 @@ def dist_init():
     return world, rank, local
 
 
+def make_reduce_max(world: int, device):
+    """max of a float over all ranks (a device tensor all-reduce; identity at world 1)."""
+    def reduce_max(x: float) -> float:
+        if world == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return reduce_max
+
+
+def replica_rate(world: int, cells_per_rank: int, steps: int, ms_local: float, reduce_max):
+    """whole-job Mcell-upd/s of `world` replicas, each advancing its own box of
+    cells_per_rank cells by `steps` steps: all ranks' cells over the slowest
+    rank's time. Returns (ms of the slowest rank, rate)."""
+    ms_max = reduce_max(ms_local)
+    return ms_max, world * cells_per_rank * steps / (ms_max / 1e3) / 1e6
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -241,13 +262,7 @@ def run_ours(args, world, rank, local):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = make_reduce_max(world, "cuda")
 
     # ---- timed region: K main-loop steps, inputs resident in HBM ----------
     clocks = ClockSampler(local)
@@ -266,8 +281,7 @@ def run_ours(args, world, rank, local):
     sim.profile(False)
     barrier()
     clk = clocks.stop()
-    ms_max = max_over_ranks(ms)
-    value = world * cells * args.steps / (ms_max / 1e3) / 1e6
+    ms_max, value = replica_rate(world, cells, args.steps, ms, max_over_ranks)
 
     # ---- roofline of the dominant kernel ------------------------------------
     hbm, hbm_kind = peaks()
