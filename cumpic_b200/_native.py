@@ -29,6 +29,8 @@ HLL = 2
 FP64, MIXED = 0, 1
 MODEL_NONE, MODEL_RIEMANN, MODEL_TORUS_SPH, MODEL_TORUS_CYN = 0, 1, 2, 3
 
+OBJ_MAGNETIC, OBJ_KINETIC, OBJ_LINEAR = 1, 2, 3
+
 K_SWEEP_X, K_SWEEP_Y, K_SWEEP_Z, K_EMF, K_COMBINE, K_UTOP, K_BOUNDARY, K_FINDDT = range(8)
 K_NAMES = ["sweep_x", "sweep_y", "sweep_z", "emf", "combine", "utop", "boundary", "finddt"]
 
@@ -69,7 +71,7 @@ EXPORTS = [
     "cumc_init", "cumc_free", "cumc_last_error", "cumc_upload_state", "cumc_download_state",
     "cumc_initial_update", "cumc_finddt", "cumc_rungekutta", "cumc_spatial", "cumc_download_lrk",
     "cumc_divb", "cumc_advance", "cumc_get_stream", "cumc_profile", "cumc_profile_read",
-    "cumc_launch_count", "cumc_cfl_dt_static", "cumc_cfl_dt_static_error",
+    "cumc_launch_count", "cumc_cfl_dt_static", "cumc_cfl_dt_static_error", "cumc_adjoint_run",
 ]
 
 
@@ -101,6 +103,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                                                                    c_double, c_double, c_void_p,
                                                                                    c_void_p]),
         "cumc_cfl_dt_static_error": (c_char_p, []),
+        "cumc_adjoint_run": (c_int, [c_void_p, c_int, c_int, c_int, dp, dp, dp, dp, dp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

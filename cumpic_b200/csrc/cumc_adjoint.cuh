@@ -1,0 +1,840 @@
+// cumc_adjoint.cuh — hand-written discrete adjoint of the FP64 RK3 step
+// (Cartesian, models NONE and RIEMANN, PPM or TVD reconstruction, HLL, CT,
+// every boundary flag).
+//
+// The forward stage s (solver/rungekutta.f90:38-66 and the kernels of
+// cumc_kernels.cuh) is, per stage,
+//   P_{s-1}   primitives with ghosts (utop + boundary of the previous combine)
+//   F         = sweeps(P_{s-1})             face fluxes (PPM/TVD + HLL)
+//   E         = emf(F, P_{s-1})             edge EMFs
+//   L         = combine's flux difference and CT curl of (F, E)
+//   Upre_s    = a U0 + b U_{s-1} + c dt L   on (0:n)^3
+//   (U_s,P_s) = utop(Upre_s) + boundary
+// with dt frozen (recorded in the forward pass). The reverse sweep of a stage
+// applies the transposes in the opposite order:
+//   boundary^T   ghost adjoints folded onto the active cells they copy
+//   utop^T       adjoint of Upre_s from those of U_s and P_s
+//   combine^T    a, b parts to U0, U_{s-1}; c dt part to L
+//   CT^T, emf^T  edge and cell-EMF adjoints
+//   sweep^T      HLL^T and PPM^T per face, limiter and solver branches
+//                frozen by recomputing the forward values
+// Cells outside 1:n and face fields outside their live positions are
+// overwritten by the forward boundary, so their adjoints are folded onto
+// their sources and then zero.
+#pragma once
+#include "cumc_kernels.cuh"
+
+namespace cumc {
+
+// device pointer sets passed by value
+struct Arr8 {
+    double* a[8];
+};
+struct Arr3 {
+    double* a[3];
+};
+
+// adjoint of the primitive fields of one stage (with ghosts)
+struct AdjPrim {
+    double* w[5];   // rho, vx, vy, vz, p
+    double* bc[3];  // cell-centred B
+    double* eps;
+};
+
+// ---------------------------------------------------------------------------
+// reconstruction transposes (branches frozen by recomputation)
+// ---------------------------------------------------------------------------
+
+// d slope / d(vm, vc, vp) of ppm_slope, times lam, added to l[0..2]
+__device__ __forceinline__ void ppm_slope_adj(double vm, double vc, double vp, double b0, double b1, double lam,
+                                              double& lm, double& lc, double& lp) {
+    if (lam == 0.0) return;
+    const double delta = b0 * (vp - vc) + b1 * (vc - vm);
+    if (!((vp - vc) * (vc - vm) > 0.0)) return;
+    const double m1 = fabs(delta), m2 = 2.0 * fabs(vc - vm), m3 = 2.0 * fabs(vc - vp);
+    const double sd = copysign(1.0, delta);
+    const double m12 = fmin(m1, m2);
+    const int sel = m12 <= m3 ? (m1 <= m2 ? 1 : 2) : 3;
+    if (sel == 1) {  // slope = delta
+        lp += b0 * lam;
+        lc += (b1 - b0) * lam;
+        lm -= b1 * lam;
+    } else if (sel == 2) {  // slope = sd * 2 |vc - vm|
+        const double g = sd * 2.0 * copysign(1.0, vc - vm) * lam;
+        lc += g;
+        lm -= g;
+    } else {  // slope = sd * 2 |vc - vp|
+        const double g = sd * 2.0 * copysign(1.0, vc - vp) * lam;
+        lc += g;
+        lp -= g;
+    }
+}
+
+// transpose of the reconstruction of one cell from v[0..4] = cells c-2..c+2:
+// seeds lvm, lvp on (vm_out, vp_out); adds to lv[0..4]
+template <int RECON>
+__device__ __forceinline__ void recon_adj(const AxisTabs& A, int c, const double v[5], double lvm, double lvp,
+                                          double lv[5]) {
+    if (lvm == 0.0 && lvp == 0.0) return;
+    if (RECON == 4) {
+        const double dmm = ppm_slope(v[0], v[1], v[2], A.s0[c - 1], A.s1[c - 1]);
+        const double dmc = ppm_slope(v[1], v[2], v[3], A.s0[c], A.s1[c]);
+        const double dmp = ppm_slope(v[2], v[3], v[4], A.s0[c + 1], A.s1[c + 1]);
+        const double vl = ppm_face(v[1], v[2], dmm, dmc, A.a0[c - 1], A.a1[c - 1], A.a2[c - 1], A.a3[c - 1]);
+        const double vr = ppm_face(v[2], v[3], dmc, dmp, A.a0[c], A.a1[c], A.a2[c], A.a3[c]);
+        const double vc = v[2];
+        // ppm_fix transpose
+        double lvc = 0.0, lvl = 0.0, lvr = 0.0;
+        if ((vr - vc) * (vc - vl) <= 0.0) {
+            lvc += lvm + lvp;
+        } else {
+            double vm1 = vl;
+            if ((vr - vl) * ((vl - 3.0 * vc) + 2.0 * vr) < 0.0) {
+                vm1 = 3.0 * vc - 2.0 * vr;
+                lvc += 3.0 * lvm;
+                lvr -= 2.0 * lvm;
+            } else {
+                lvl += lvm;
+            }
+            if ((vr - vm1) * ((3.0 * vc - 2.0 * vl) - vr) < 0.0) {
+                lvc += 3.0 * lvp;
+                lvl -= 2.0 * lvp;
+            } else {
+                lvr += lvp;
+            }
+        }
+        // interface values: V = vc' + (a0 + a1)(vp' - vc') + a2 dmp' + a3 dmc'
+        double ldmm = 0.0, ldmc = 0.0, ldmp = 0.0;
+        {
+            const double s = A.a0[c - 1] + A.a1[c - 1];
+            lv[1] += (1.0 - s) * lvl;
+            lv[2] += s * lvl;
+            ldmc += A.a2[c - 1] * lvl;
+            ldmm += A.a3[c - 1] * lvl;
+        }
+        {
+            const double s = A.a0[c] + A.a1[c];
+            lv[2] += (1.0 - s) * lvr;
+            lv[3] += s * lvr;
+            ldmp += A.a2[c] * lvr;
+            ldmc += A.a3[c] * lvr;
+        }
+        lv[2] += lvc;
+        ppm_slope_adj(v[0], v[1], v[2], A.s0[c - 1], A.s1[c - 1], ldmm, lv[0], lv[1], lv[2]);
+        ppm_slope_adj(v[1], v[2], v[3], A.s0[c], A.s1[c], ldmc, lv[1], lv[2], lv[3]);
+        ppm_slope_adj(v[2], v[3], v[4], A.s0[c + 1], A.s1[c + 1], ldmp, lv[2], lv[3], lv[4]);
+    } else {
+        // vm = vc - sl/2, vp = vc + sl/2, sl = minmod of dqf = 2(vp-vc)/cf, dqb = 2(vc-vm)/cb
+        lv[2] += lvm + lvp;
+        const double lsl = 0.5 * (lvp - lvm);
+        const double cf = A.tcf[c], cb = A.tcb[c];
+        const double dqf = (2.0 * (v[3] - v[2])) / cf;
+        const double dqb = (2.0 * (v[2] - v[1])) / cb;
+        const double sf = copysign(1.0, dqf), sb = copysign(1.0, dqb);
+        if (sf != sb) return;  // slope 0
+        if (fabs(dqf) <= fabs(dqb)) {  // slope = dqf
+            lv[3] += 2.0 * lsl / cf;
+            lv[2] -= 2.0 * lsl / cf;
+        } else {  // slope = dqb
+            lv[2] += 2.0 * lsl / cb;
+            lv[1] -= 2.0 * lsl / cb;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// HLL transpose (hll_flux7 of cumc_device.cuh, branches frozen)
+// ---------------------------------------------------------------------------
+template <int DIR>
+struct SideAdj {
+    double rho, v[3], p, b[3], e, vsq, bsq, E, hb2, vdotb;
+    double Lrho, Lv[3], Lp, Lb[3], LE, Lhb2, Lvdotb;
+    __device__ __forceinline__ void init(const double w[8], double g) {
+        rho = w[IRHO];
+        v[0] = w[IVX]; v[1] = w[IVY]; v[2] = w[IVZ];
+        p = w[ITAU];
+        b[0] = w[IBX]; b[1] = w[IBY]; b[2] = w[IBZ];
+        e = (p / rho) / (g - 1.0);
+        vsq = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
+        bsq = (b[0] * b[0] + b[1] * b[1]) + b[2] * b[2];
+        E = rho * (e + 0.5 * vsq) + 0.5 * bsq;
+        hb2 = 0.5 * bsq;
+        vdotb = (b[0] * v[0] + b[1] * v[1]) + b[2] * v[2];
+        Lrho = Lp = LE = Lhb2 = Lvdotb = 0.0;
+        for (int i = 0; i < 3; ++i) Lv[i] = Lb[i] = 0.0;
+    }
+    __device__ __forceinline__ double u(int q) const {
+        return q == IRHO ? rho : q <= IVZ ? v[q - IVX] * rho : q == ITAU ? E : b[q - IBX];
+    }
+    __device__ __forceinline__ double f(int q) const {
+        constexpr int t1 = (DIR + 1) % 3, t2 = (DIR + 2) % 3;
+        const double vn = v[DIR], bn = b[DIR];
+        if (q == IRHO) return rho * vn;
+        if (q == IVX + DIR) return ((v[DIR] * rho * vn + p) + hb2) - bn * bn;
+        if (q == IVX + t1) return v[t1] * rho * vn - bn * b[t1];
+        if (q == IVX + t2) return v[t2] * rho * vn - bn * b[t2];
+        if (q == ITAU) return (E * vn + (p + hb2) * vn) - bn * vdotb;
+        if (q == IBX + t1) return vn * b[t1] - v[t1] * bn;
+        return vn * b[t2] - v[t2] * bn;
+    }
+    __device__ __forceinline__ void u_adj(int q, double lam) {
+        if (q == IRHO) Lrho += lam;
+        else if (q <= IVZ) { Lv[q - IVX] += lam * rho; Lrho += lam * v[q - IVX]; }
+        else if (q == ITAU) LE += lam;
+        else Lb[q - IBX] += lam;
+    }
+    __device__ __forceinline__ void f_adj(int q, double lam) {
+        const double vn = v[DIR], bn = b[DIR];
+        if (q == IRHO) {
+            Lrho += lam * vn;
+            Lv[DIR] += lam * rho;
+        } else if (q == IVX + DIR) {
+            Lv[DIR] += lam * 2.0 * rho * vn;
+            Lrho += lam * vn * vn;
+            Lp += lam;
+            Lhb2 += lam;
+            Lb[DIR] -= lam * 2.0 * bn;
+        } else if (q >= IVX && q <= IVZ) {
+            const int t = q - IVX;
+            Lv[t] += lam * rho * vn;
+            Lrho += lam * v[t] * vn;
+            Lv[DIR] += lam * v[t] * rho;
+            Lb[DIR] -= lam * b[t];
+            Lb[t] -= lam * bn;
+        } else if (q == ITAU) {
+            LE += lam * vn;
+            Lv[DIR] += lam * (E + p + hb2);
+            Lp += lam * vn;
+            Lhb2 += lam * vn;
+            Lb[DIR] -= lam * vdotb;
+            Lvdotb -= lam * bn;
+        } else {
+            const int t = q - IBX;
+            Lv[DIR] += lam * b[t];
+            Lb[t] += lam * vn;
+            Lv[t] -= lam * bn;
+            Lb[DIR] -= lam * v[t];
+        }
+    }
+    // fold E, hb2, vdotb, e into the primitive adjoints; out[8] in natural order
+    __device__ __forceinline__ void finish(double g, double out[8]) {
+        const double Le = LE * rho;
+        const double Lvsq = LE * 0.5 * rho;
+        const double Lbsq = LE * 0.5 + 0.5 * Lhb2;
+        Lrho += LE * (e + 0.5 * vsq);
+        for (int i = 0; i < 3; ++i) {
+            Lb[i] += Lvdotb * v[i] + 2.0 * b[i] * Lbsq;
+            Lv[i] += Lvdotb * b[i] + 2.0 * v[i] * Lvsq;
+        }
+        Lp += Le / (rho * (g - 1.0));
+        Lrho -= Le * e / rho;
+        out[IRHO] += Lrho;
+        out[IVX] += Lv[0]; out[IVY] += Lv[1]; out[IVZ] += Lv[2];
+        out[ITAU] += Lp;
+        out[IBX] += Lb[0]; out[IBY] += Lb[1]; out[IBZ] += Lb[2];
+    }
+};
+
+// adjoint of cf = signalspeed(cs, bn, bt1, bt2, rho): adds to the arguments' adjoints
+__device__ __forceinline__ void signalspeed_adj(double cs, double bn, double bt1, double bt2, double rho, double lcf,
+                                                double& lcs, double& lbn, double& lbt1, double& lbt2, double& lrho) {
+    if (lcf == 0.0) return;
+    const double a2 = cs * cs;
+    const double b2n = (bn * bn) / rho, b2t1 = (bt1 * bt1) / rho, b2t2 = (bt2 * bt2) / rho;
+    const double b2 = (b2n + b2t1) + b2t2;
+    const double inner = ((a2 * a2 + b2 * b2) + (2.0 * b2) * a2) - (4.0 * a2) * b2n;
+    const double s = sqrt(fmax(inner, 0.0));
+    const double cf = sqrt(0.5 * ((a2 + b2) + s));
+    if (!(cf > 0.0)) return;
+    const double lsum = lcf * 0.25 / cf;  // d cf / d (a2 + b2 + s)
+    double la2 = lsum, lb2 = lsum, lb2n = 0.0;
+    if (inner > 0.0) {
+        const double ls = lsum / (2.0 * s);  // d s / d inner
+        la2 += ls * (2.0 * (a2 + b2) - 4.0 * b2n);
+        lb2 += ls * 2.0 * (a2 + b2);
+        lb2n += ls * (-4.0 * a2);
+    }
+    lb2n += lb2;
+    lcs += 2.0 * cs * la2;
+    lbn += 2.0 * bn / rho * lb2n;
+    lbt1 += 2.0 * bt1 / rho * lb2;
+    lbt2 += 2.0 * bt2 / rho * lb2;
+    lrho -= (b2n * lb2n + (b2t1 + b2t2) * lb2) / rho;
+}
+
+// adjoint of out[7] = hll_flux7<DIR>(wl, wr): lout[7] -> lwl[8], lwr[8] (added)
+template <int DIR>
+__device__ __forceinline__ void hll_adj(const double wl[8], const double wr[8], double g, const double lout[7],
+                                        double lwl[8], double lwr[8]) {
+    constexpr int ivn = IVX + DIR;
+    constexpr int ibn = IBX + DIR, ibt1 = IBX + (DIR + 1) % 3, ibt2 = IBX + (DIR + 2) % 3;
+    constexpr int bt_a = DIR == 0 ? IBY : IBX;
+    constexpr int bt_b = DIR == 2 ? IBY : IBZ;
+    const int comp[7] = {IRHO, IVX, IVY, IVZ, ITAU, bt_a, bt_b};
+    SideAdj<DIR> L, R;
+    L.init(wl, g);
+    R.init(wr, g);
+    const double csL = sqrt((g * wl[ITAU]) / wl[IRHO]);
+    const double csR = sqrt((g * wr[ITAU]) / wr[IRHO]);
+    const double cfL = signalspeed(csL, wl[ibn], wl[ibt1], wl[ibt2], wl[IRHO]);
+    const double cfR = signalspeed(csR, wr[ibn], wr[ibt1], wr[ibt2], wr[IRHO]);
+    const double sqL = sqrt(wl[IRHO]), sqR = sqrt(wr[IRHO]);
+    const double ubar = roe_avg(wl[ivn], wr[ivn], sqL, sqR);
+    const double cbar = roe_avg(cfL, cfR, sqL, sqR);
+    const double aL = wl[ivn] - cfL, bL = ubar - cbar;
+    const double aR = wr[ivn] + cfR, bR = ubar + cbar;
+    const double sL = fmin(aL, bL), sR = fmax(aR, bR);
+    double lsL = 0.0, lsR = 0.0;
+    if (sL >= 0.0) {
+        for (int c = 0; c < 7; ++c) L.f_adj(comp[c], lout[c]);
+    } else if (sL <= 0.0 && sR >= 0.0) {
+        const double d = sR - sL;
+        double ld = 0.0;
+        for (int c = 0; c < 7; ++c) {
+            const int q = comp[c];
+            const double fl = L.f(q), fr = R.f(q), ul = L.u(q), ur = R.u(q);
+            const double out = ((sR * fl - sL * fr) + (sL * sR) * (ur - ul)) / d;
+            const double ln = lout[c] / d;
+            ld -= lout[c] * out / d;
+            L.f_adj(q, sR * ln);
+            R.f_adj(q, -sL * ln);
+            R.u_adj(q, sL * sR * ln);
+            L.u_adj(q, -sL * sR * ln);
+            lsR += ln * (fl + sL * (ur - ul));
+            lsL += ln * (-fr + sR * (ur - ul));
+        }
+        lsR += ld;
+        lsL -= ld;
+    } else {
+        for (int c = 0; c < 7; ++c) R.f_adj(comp[c], lout[c]);
+    }
+    // sL = min(aL, bL), sR = max(aR, bR)
+    double lvnL = 0.0, lvnR = 0.0, lcfL = 0.0, lcfR = 0.0, lubar = 0.0, lcbar = 0.0;
+    if (aL <= bL) { lvnL += lsL; lcfL -= lsL; } else { lubar += lsL; lcbar -= lsL; }
+    if (aR >= bR) { lvnR += lsR; lcfR += lsR; } else { lubar += lsR; lcbar += lsR; }
+    // Roe averages
+    const double ssum = sqL + sqR;
+    double lsqL = (lubar * (wl[ivn] - ubar) + lcbar * (cfL - cbar)) / ssum;
+    double lsqR = (lubar * (wr[ivn] - ubar) + lcbar * (cfR - cbar)) / ssum;
+    lvnL += lubar * sqL / ssum;
+    lvnR += lubar * sqR / ssum;
+    lcfL += lcbar * sqL / ssum;
+    lcfR += lcbar * sqR / ssum;
+    // fast speeds
+    double lcsL = 0.0, lcsR = 0.0;
+    signalspeed_adj(csL, wl[ibn], wl[ibt1], wl[ibt2], wl[IRHO], lcfL, lcsL, L.Lb[DIR], L.Lb[(DIR + 1) % 3],
+                    L.Lb[(DIR + 2) % 3], L.Lrho);
+    signalspeed_adj(csR, wr[ibn], wr[ibt1], wr[ibt2], wr[IRHO], lcfR, lcsR, R.Lb[DIR], R.Lb[(DIR + 1) % 3],
+                    R.Lb[(DIR + 2) % 3], R.Lrho);
+    // cs = sqrt(g p / rho), sq = sqrt(rho)
+    if (csL > 0.0) {
+        L.Lp += lcsL * g / (2.0 * csL * wl[IRHO]);
+        L.Lrho -= lcsL * csL / (2.0 * wl[IRHO]);
+    }
+    if (csR > 0.0) {
+        R.Lp += lcsR * g / (2.0 * csR * wr[IRHO]);
+        R.Lrho -= lcsR * csR / (2.0 * wr[IRHO]);
+    }
+    L.Lrho += lsqL / (2.0 * sqL);
+    R.Lrho += lsqR / (2.0 * sqR);
+    L.Lv[DIR] += lvnL;
+    R.Lv[DIR] += lvnR;
+    L.finish(g, lwl);
+    R.finish(g, lwr);
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+struct AdjStage {
+    const double* mu[8];    // adjoint of the combine's output (Upre), live entries only
+    const double* lamE[3];  // edge-EMF adjoints (k_adj_ct)
+    const double* dt;       // device dt of the step
+    double gam;             // combine's coefficient on dt L
+};
+
+__device__ __forceinline__ bool inside(int j, int k, int l, const Box& b) {
+    return j >= 1 && j <= b.nx && k >= 1 && k <= b.ny && l >= 1 && l <= b.nz;
+}
+__device__ __forceinline__ bool in0n(int j, int k, int l, const Box& b) {
+    return j >= 0 && j <= b.nx && k >= 0 && k <= b.ny && l >= 0 && l <= b.nz;
+}
+
+// CT^T: edge-EMF adjoints on (0:n)^3 from the field part of mu (solver/mhd.f90:137-148)
+__global__ void __launch_bounds__(256) k_adj_ct(Box b, Tabs T, AdjStage a, double* lex, double* ley, double* lez) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int j = (int)(t % n0), k = (int)((t / n0) % n1), l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
+    const double cdt = a.gam * *a.dt;
+    const double* mx = a.mu[IBX];
+    const double* my = a.mu[IBY];
+    const double* mz = a.mu[IBZ];
+    const double dx0 = T.ax[0].d[j], dy0 = T.ax[1].d[k], dz0 = T.ax[2].d[l];
+    const bool jp = j + 1 <= b.nx, kp = k + 1 <= b.ny, lp = l + 1 <= b.nz;
+    const double dx1 = T.ax[0].d[j + 1], dy1 = T.ax[1].d[k + 1], dz1 = T.ax[2].d[l + 1];
+    double ez = -mx[i] / dy0 + my[i] / dx0;
+    if (kp) ez += mx[i + sk] / dy1;
+    if (jp) ez -= my[i + sj] / dx1;
+    double ey = mx[i] / dz0 - mz[i] / dx0;
+    if (lp) ey -= mx[i + sl] / dz1;
+    if (jp) ey += mz[i + sj] / dx1;
+    double ex = -my[i] / dz0 + mz[i] / dy0;
+    if (lp) ex += my[i + sl] / dz1;
+    if (kp) ex -= mz[i + sk] / dy1;
+    lex[i] = cdt * ex;
+    ley[i] = cdt * ey;
+    lez[i] = cdt * ez;
+}
+
+// emf^T, cell part: ecell = -v x B on (0:n+1)^3 enters four edges with -1/4
+// (solver/mhd.f90:95-125); adds to the velocity and cell-field adjoints
+__global__ void __launch_bounds__(256) k_adj_ecell(Box b, Prim pr, const double* lex, const double* ley,
+                                                   const double* lez, AdjPrim o) {
+    const int n0 = b.nx + 2, n1 = b.ny + 2, n2 = b.nz + 2;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int j = (int)(t % n0), k = (int)((t / n0) % n1), l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
+    auto E = [&](const double* e, int dj, int dk, int dl) -> double {
+        const int jj = j - dj, kk = k - dk, ll = l - dl;
+        return in0n(jj, kk, ll, b) ? e[i - dj * sj - dk * sk - dl * sl] : 0.0;
+    };
+    const double lx = -0.25 * (((E(lex, 0, 0, 0) + E(lex, 0, 0, 1)) + E(lex, 0, 1, 0)) + E(lex, 0, 1, 1));
+    const double ly = -0.25 * (((E(ley, 0, 0, 0) + E(ley, 0, 0, 1)) + E(ley, 1, 0, 0)) + E(ley, 1, 0, 1));
+    const double lz = -0.25 * (((E(lez, 0, 0, 0) + E(lez, 0, 1, 0)) + E(lez, 1, 0, 0)) + E(lez, 1, 1, 0));
+    if (lx == 0.0 && ly == 0.0 && lz == 0.0) return;
+    const double vx = pr.w[1][i], vy = pr.w[2][i], vz = pr.w[3][i];
+    const double bx = pr.bc[0][i], by = pr.bc[1][i], bz = pr.bc[2][i];
+    // ex = vz by - vy bz, ey = vx bz - vz bx, ez = vy bx - vx by
+    o.w[1][i] += ly * bz - lz * by;
+    o.w[2][i] += lz * bx - lx * bz;
+    o.w[3][i] += lx * by - ly * bx;
+    o.bc[0][i] += lz * vy - ly * vz;
+    o.bc[1][i] += lx * vz - lz * vx;
+    o.bc[2][i] += ly * vx - lx * vy;
+}
+
+// sweep^T: per face (normal 0:n_d, transverse 0:n+1), the flux adjoints from
+// mu (flux difference) and the edge adjoints (emf), then HLL^T and the
+// reconstruction transposes of the two adjacent cells, accumulated into the
+// primitive adjoints of cells c-2..c+3 (atomically: neighbouring faces share
+// cells) and into the normal-field adjoint of the face (lambf).
+template <int DIR, int RECON>
+__global__ void __launch_bounds__(128) k_adj_sweep(Box b, Tabs T, Prim pr, double ggas, AdjStage a, AdjPrim o,
+                                                  double* lambf) {
+    const int n0 = (DIR == 0 ? b.nx : b.nx + 1) + 1;
+    const int n1 = (DIR == 1 ? b.ny : b.ny + 1) + 1;
+    const int n2 = (DIR == 2 ? b.nz : b.nz + 1) + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int j = (int)(t % n0), k = (int)((t / n0) % n1), l = (int)(t / ((long long)n0 * n1));
+    const int base = b.idx(j, k, l);
+    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
+    const int s = DIR == 0 ? sj : DIR == 1 ? sk : sl;
+    const int c = DIR == 0 ? j : DIR == 1 ? k : l;
+    const int nd = DIR == 0 ? b.nx : DIR == 1 ? b.ny : b.nz;
+    const AxisTabs A = T.ax[DIR];
+
+    // flux adjoints
+    double lf[7];
+    const double cdt = a.gam * *a.dt;
+    {
+        const bool tin = DIR == 0 ? (k >= 1 && k <= b.ny && l >= 1 && l <= b.nz)
+                                  : DIR == 1 ? (j >= 1 && j <= b.nx && l >= 1 && l <= b.nz)
+                                             : (j >= 1 && j <= b.nx && k >= 1 && k <= b.ny);
+        const bool lin = tin && c >= 1, rin = tin && c + 1 <= nd;
+        const double il = lin ? 1.0 / A.d[c] : 0.0, ir = rin ? 1.0 / A.d[c + 1] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double ml = lin ? a.mu[q][base] : 0.0, mr = rin ? a.mu[q][base + s] : 0.0;
+            lf[q] = cdt * (mr * ir - ml * il);
+        }
+        auto E = [&](const double* e, int dj, int dk, int dl) -> double {
+            return in0n(j - dj, k - dk, l - dl, b) ? e[base - dj * sj - dk * sk - dl * sl] : 0.0;
+        };
+        if (DIR == 0) {  // x faces: by enters ez (-1/2), bz enters ey (+1/2)
+            lf[5] = -0.5 * (E(a.lamE[2], 0, 0, 0) + E(a.lamE[2], 0, 1, 0));
+            lf[6] = 0.5 * (E(a.lamE[1], 0, 0, 0) + E(a.lamE[1], 0, 0, 1));
+        } else if (DIR == 1) {  // y faces: bx enters ez (+1/2), bz enters ex (-1/2)
+            lf[5] = 0.5 * (E(a.lamE[2], 0, 0, 0) + E(a.lamE[2], 1, 0, 0));
+            lf[6] = -0.5 * (E(a.lamE[0], 0, 0, 0) + E(a.lamE[0], 0, 0, 1));
+        } else {  // z faces: bx enters ey (-1/2), by enters ex (+1/2)
+            lf[5] = -0.5 * (E(a.lamE[1], 0, 0, 0) + E(a.lamE[1], 1, 0, 0));
+            lf[6] = 0.5 * (E(a.lamE[0], 0, 0, 0) + E(a.lamE[0], 0, 1, 0));
+        }
+    }
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) any |= lf[q] != 0.0;
+    if (!any) return;
+
+    constexpr int bt_a = DIR == 0 ? 1 : 0;
+    constexpr int bt_b = DIR == 2 ? 1 : 2;
+    const double* src[7] = {pr.w[0], pr.w[1], pr.w[2], pr.w[3], pr.w[4], pr.bc[bt_a], pr.bc[bt_b]};
+    double* dst[7] = {o.w[0], o.w[1], o.w[2], o.w[3], o.w[4], o.bc[bt_a], o.bc[bt_b]};
+    const int slot[7] = {IRHO, IVX, IVY, IVZ, ITAU, IBX + bt_a, IBX + bt_b};
+
+    // forward states
+    double wl[8], wr[8], cv[7][6];
+#pragma unroll
+    for (int v = 0; v < 7; ++v) {
+        const double* q = src[v] + base;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) cv[v][m] = q[(m - 2) * s];  // cells c-2..c+3
+        double vm, vp;
+        if (RECON == 4) {
+            const double dmm = ppm_slope(cv[v][0], cv[v][1], cv[v][2], A.s0[c - 1], A.s1[c - 1]);
+            const double dmc = ppm_slope(cv[v][1], cv[v][2], cv[v][3], A.s0[c], A.s1[c]);
+            const double dmp = ppm_slope(cv[v][2], cv[v][3], cv[v][4], A.s0[c + 1], A.s1[c + 1]);
+            const double dmq = ppm_slope(cv[v][3], cv[v][4], cv[v][5], A.s0[c + 2], A.s1[c + 2]);
+            const double V0 = ppm_face(cv[v][1], cv[v][2], dmm, dmc, A.a0[c - 1], A.a1[c - 1], A.a2[c - 1], A.a3[c - 1]);
+            const double V1 = ppm_face(cv[v][2], cv[v][3], dmc, dmp, A.a0[c], A.a1[c], A.a2[c], A.a3[c]);
+            const double V2 = ppm_face(cv[v][3], cv[v][4], dmp, dmq, A.a0[c + 1], A.a1[c + 1], A.a2[c + 1], A.a3[c + 1]);
+            double vm0, vp1;
+            ppm_fix(cv[v][2], V0, V1, vm0, vp);
+            ppm_fix(cv[v][3], V1, V2, vm, vp1);
+        } else {
+            vp = cv[v][2] + 0.5 * tvd_slope(cv[v][1], cv[v][2], cv[v][3], A.tcf[c], A.tcb[c]);
+            vm = cv[v][3] - 0.5 * tvd_slope(cv[v][2], cv[v][3], cv[v][4], A.tcf[c + 1], A.tcb[c + 1]);
+        }
+        wl[slot[v]] = vp;
+        wr[slot[v]] = vm;
+    }
+    const double bn = pr.bf[DIR][base];
+    wl[IBX + DIR] = bn;
+    wr[IBX + DIR] = bn;
+
+    double lwl[8] = {0, 0, 0, 0, 0, 0, 0, 0}, lwr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    hll_adj<DIR>(wl, wr, ggas, lf, lwl, lwr);
+    lambf[base] += lwl[IBX + DIR] + lwr[IBX + DIR];
+
+#pragma unroll
+    for (int v = 0; v < 7; ++v) {
+        double lv[6] = {0, 0, 0, 0, 0, 0};
+        recon_adj<RECON>(A, c, &cv[v][0], 0.0, lwl[slot[v]], &lv[0]);      // vp_out of cell c
+        recon_adj<RECON>(A, c + 1, &cv[v][1], lwr[slot[v]], 0.0, &lv[1]);  // vm_out of cell c+1
+#pragma unroll
+        for (int m = 0; m < 6; ++m)
+            if (lv[m] != 0.0) atomicAdd(dst[v] + base + (m - 2) * s, lv[m]);
+    }
+}
+
+// boundary^T: the transpose of k_boundary. Each ghost's adjoint (after the
+// ghost-pressure term p = rho eps (gamma-1), solver/update.f90:27-35) is added,
+// with the parity sign, to the active cell (or live face) it was copied from,
+// then cleared. Several ghosts share a source (corners, outflow copies), so
+// the additions are atomic. fw holds the forward primitives of the stage.
+__global__ void __launch_bounds__(256) k_adj_boundary(Box b, BoundArgs fw, AdjPrim o, double* lbx, double* lby,
+                                                      double* lbz) {
+    const long long zsl = 6LL * b.SX * b.SY, ysl = 6LL * b.SX * b.nz, xsl = 6LL * b.ny * b.nz;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int j, k, l;
+    if (t < zsl) {
+        const int s = (int)(t / ((long long)b.SX * b.SY));
+        const int r = (int)(t % ((long long)b.SX * b.SY));
+        l = s < 3 ? s - 2 : b.nz + s - 2;
+        k = r / b.SX - 2;
+        j = r % b.SX - 2;
+    } else if ((t -= zsl) < ysl) {
+        const int s = (int)(t / ((long long)b.SX * b.nz));
+        const int r = (int)(t % ((long long)b.SX * b.nz));
+        k = s < 3 ? s - 2 : b.ny + s - 2;
+        l = r / b.SX + 1;
+        j = r % b.SX - 2;
+    } else if ((t -= ysl) < xsl) {
+        const int s = (int)(t / ((long long)b.ny * b.nz));
+        const int r = (int)(t % ((long long)b.ny * b.nz));
+        j = s < 3 ? s - 2 : b.nx + s - 2;
+        l = r / b.ny + 1;
+        k = r % b.ny + 1;
+    } else {
+        return;
+    }
+    const int i = b.idx(j, k, l);
+    int sj, sk, sl, dj, dk, dl;
+    const bool gx = gmap(j, b.nx, fw.flag[0], fw.flag[1], sj, dj);
+    const bool gy = gmap(k, b.ny, fw.flag[2], fw.flag[3], sk, dk);
+    const bool gz = gmap(l, b.nz, fw.flag[4], fw.flag[5], sl, dl);
+    auto sgn = [&](int q) -> double {
+        int s = 1;
+        if (gx && fw.flag[dj] >= 2) s *= fw.fac[dj][q];
+        if (gy && fw.flag[2 + dk] >= 2) s *= fw.fac[2 + dk][q];
+        if (gz && fw.flag[4 + dl] >= 2) s *= fw.fac[4 + dl][q];
+        return (double)s;
+    };
+    const int src = b.idx(sj, sk, sl);
+    // ghost pressure
+    const double lp = o.w[4][i];
+    o.w[4][i] = 0.0;
+    double lrho = o.w[0][i] + lp * fw.eps[i] * (fw.ggas - 1.0);
+    double leps = o.eps[i] + lp * fw.w[0][i] * (fw.ggas - 1.0);
+    const double lw[4] = {lrho, o.w[1][i], o.w[2][i], o.w[3][i]};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        o.w[q][i] = 0.0;
+        if (lw[q] != 0.0) atomicAdd(o.w[q] + src, sgn(q) * lw[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double v = o.bc[q][i];
+        o.bc[q][i] = 0.0;
+        if (v != 0.0) atomicAdd(o.bc[q] + src, sgn(IBX + q) * v);
+    }
+    {
+        int ej = j, ek = k, el = l, dd;
+        gmap(j, b.nx, fw.flag[0], fw.flag[1], ej, dd);
+        gmap(k, b.ny, fw.flag[2], fw.eps_yout, ek, dd);
+        gmap(l, b.nz, fw.flag[4], fw.flag[5], el, dd);
+        o.eps[i] = 0.0;
+        if (leps != 0.0) atomicAdd(o.eps + b.idx(ej, ek, el), leps);
+    }
+    if (j >= 0 && j <= b.nx && (gy || gz)) {
+        int s = 1;
+        if (gy && fw.flag[2 + dk] >= 2) s *= fw.fac[2 + dk][IBX];
+        if (gz && fw.flag[4 + dl] >= 2) s *= fw.fac[4 + dl][IBX];
+        const double v = lbx[i];
+        lbx[i] = 0.0;
+        if (v != 0.0) atomicAdd(lbx + b.idx(j, sk, sl), s * v);
+    }
+    if (k >= 0 && k <= b.ny && (gx || gz)) {
+        int s = 1;
+        if (gx && fw.flag[dj] >= 2) s *= fw.fac[dj][IBY];
+        if (gz && fw.flag[4 + dl] >= 2) s *= fw.fac[4 + dl][IBY];
+        const double v = lby[i];
+        lby[i] = 0.0;
+        if (v != 0.0) atomicAdd(lby + b.idx(sj, k, sl), s * v);
+    }
+    if (l >= 0 && l <= b.nz && (gx || gy)) {
+        int s = 1;
+        if (gx && fw.flag[dj] >= 2) s *= fw.fac[dj][IBZ];
+        if (gy && fw.flag[2 + dk] >= 2) s *= fw.fac[2 + dk][IBZ];
+        const double v = lbz[i];
+        lbz[i] = 0.0;
+        if (v != 0.0) atomicAdd(lbz + b.idx(sj, sk, l), s * v);
+    }
+}
+
+// utop^T on the active cells: from the adjoints of the re-derived conserved
+// hydro variables (lu) and of the primitives (o), the adjoint of the
+// combine's output Upre (hydro part, mu) and of the cell-centred field
+// (lb, folded onto the faces by k_adj_bface). FROMUTORVE, CHECKRHO (RIEMANN:
+// eps >= 0, branch frozen), FROMRVETOU and UPDATE's pressure
+// (solver/fromrvetou.f90:21-127, solver/update.f90:27-35). FROM_CONS=false is
+// initial_update, whose inputs are the uploaded rho, v and eps: mu then
+// receives (rho, vx, vy, vz, eps) adjoints.
+template <int MODEL, bool FROM_CONS>
+__global__ void __launch_bounds__(256) k_adj_utop(Box b, Arr8 u, Arr8 w0, const double* eps0, Arr8 lu,
+                                                  AdjPrim o, double ggas, Arr8 mu, Arr3 lb) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int j = (int)(t % n0), k = (int)((t / n0) % n1), l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    if (!(j >= 1 && k >= 1 && l >= 1)) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) mu.a[q][i] = 0.0;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) lb.a[q][i] = 0.0;
+        return;
+    }
+    const double bx = 0.5 * (u.a[IBX][i] + u.a[IBX][i - 1]);
+    const double by = 0.5 * (u.a[IBY][i] + u.a[IBY][i - b.SX]);
+    const double bz = 0.5 * (u.a[IBZ][i] + u.a[IBZ][i - b.SX * b.SY]);
+    const double bsquare = (bx * bx + by * by) + bz * bz;
+    double rho, vx, vy, vz, e_raw;
+    if (FROM_CONS) {
+        rho = u.a[IRHO][i];
+        vx = u.a[IVX][i] / rho;
+        vy = u.a[IVY][i] / rho;
+        vz = u.a[IVZ][i] / rho;
+        const double vsq = (vx * vx + vy * vy) + vz * vz;
+        e_raw = (u.a[ITAU][i] - 0.5 * bsquare) / rho - 0.5 * vsq;
+    } else {
+        rho = w0.a[0][i];
+        vx = w0.a[1][i];
+        vy = w0.a[2][i];
+        vz = w0.a[3][i];
+        e_raw = eps0[i];
+    }
+    const bool clamped = MODEL == 1 && !(e_raw >= 0.0);
+    const double e = clamped ? 0.0 : e_raw;
+    const double vsquare = (vx * vx + vy * vy) + vz * vz;
+    const double g1 = ggas - 1.0;
+    // adjoint inputs
+    const double lu0 = lu.a[IRHO][i], lu1 = lu.a[IVX][i], lu2 = lu.a[IVY][i], lu3 = lu.a[IVZ][i], lu4 = lu.a[ITAU][i];
+    const double lp = o.w[4][i];
+    double Lrho = lu0 + o.w[0][i] + lu1 * vx + lu2 * vy + lu3 * vz + lu4 * (e + 0.5 * vsquare) + lp * e * g1;
+    double Lvx = o.w[1][i] + lu1 * rho, Lvy = o.w[2][i] + lu2 * rho, Lvz = o.w[3][i] + lu3 * rho;
+    double Le = o.eps[i] + lu4 * rho + lp * rho * g1;
+    double Lvsq = lu4 * 0.5 * rho;
+    double Lbsq = 0.5 * lu4;
+    if (clamped) Le = 0.0;
+    if (FROM_CONS) {
+        // e_raw = (E - bsq/2)/rho - vsq/2
+        const double E = u.a[ITAU][i];
+        const double LE = Le / rho;
+        Lbsq -= 0.5 * Le / rho;
+        Lrho -= Le * (E - 0.5 * bsquare) / (rho * rho);
+        Lvsq -= 0.5 * Le;
+        Lvx += 2.0 * vx * Lvsq;
+        Lvy += 2.0 * vy * Lvsq;
+        Lvz += 2.0 * vz * Lvsq;
+        // v = m / rho
+        mu.a[IVX][i] = Lvx / rho;
+        mu.a[IVY][i] = Lvy / rho;
+        mu.a[IVZ][i] = Lvz / rho;
+        Lrho -= (Lvx * vx + Lvy * vy + Lvz * vz) / rho;
+        mu.a[IRHO][i] = Lrho;
+        mu.a[ITAU][i] = LE;
+    } else {
+        Lvx += 2.0 * vx * Lvsq;
+        Lvy += 2.0 * vy * Lvsq;
+        Lvz += 2.0 * vz * Lvsq;
+        mu.a[0][i] = Lrho;
+        mu.a[1][i] = Lvx;
+        mu.a[2][i] = Lvy;
+        mu.a[3][i] = Lvz;
+        mu.a[4][i] = Le;  // adjoint of the uploaded eps
+    }
+    lb.a[0][i] = o.bc[0][i] + 2.0 * bx * Lbsq;
+    lb.a[1][i] = o.bc[1][i] + 2.0 * by * Lbsq;
+    lb.a[2][i] = o.bc[2][i] + 2.0 * bz * Lbsq;
+}
+
+// face-field adjoint on (0:n)^3: the pass-through adjoint of the live face
+// values plus half the adjoints of the two active cells whose bcell average
+// reads the face (solver/fromrvetou.f90:97-107); zero on every other entry
+__global__ void __launch_bounds__(256) k_adj_bface(Box b, Arr3 lbf, Arr3 lb, Arr3 out) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int j = (int)(t % n0), k = (int)((t / n0) % n1), l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const int st[3] = {1, b.SX, b.SX * b.SY};
+    const int own[3] = {j, k, l};
+    const int nn[3] = {b.nx, b.ny, b.nz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        bool live = true;
+#pragma unroll
+        for (int e = 0; e < 3; ++e)
+            if (e != d && (own[e] < 1 || own[e] > nn[e])) live = false;
+        double v = 0.0;
+        if (live) {
+            v = lbf.a[d][i];
+            const double left = own[d] >= 1 ? lb.a[d][i] : 0.0;
+            const double right = own[d] + 1 <= nn[d] ? lb.a[d][i + st[d]] : 0.0;
+            v += 0.5 * (left + right);
+        }
+        out.a[d][i] = v;
+    }
+}
+
+// combine^T, elementwise over the box: lamU0 += a mu, lamCur = b mu (b = 0:
+// left alone). mu is zero off the live entries.
+__global__ void __launch_bounds__(256) k_adj_combine(long long n, Arr8 mu, double a, double bco, Arr8 lam0,
+                                                     Arr8 lamc) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const double m = mu.a[q][t];
+        lam0.a[q][t] += a * m;
+        if (bco != 0.0) lamc.a[q][t] = bco * m;
+    }
+}
+
+// objective at the final state, per-block partial sums (deterministic order)
+// and its adjoint seed. kind 1: magnetic energy 0.5 sum |bcell|^2 dV; kind 2:
+// kinetic energy 0.5 sum rho |v|^2 dV; kind 3: sum of weights . cons over the
+// live entries (weights in lamu on entry).
+__global__ void __launch_bounds__(256) k_adj_objective(Box b, Tabs T, Prim pr, Arr8 u, int kind, AdjPrim o,
+                                                       Arr8 lamu, double* partial) {
+    const long long total = (long long)b.nx * b.ny * b.nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double acc = 0.0;
+    if (t < total) {
+        const int j = (int)(t % b.nx) + 1, k = (int)((t / b.nx) % b.ny) + 1, l = (int)(t / ((long long)b.nx * b.ny)) + 1;
+        const int i = b.idx(j, k, l);
+        const double dv = (T.ax[0].d[j] * T.ax[1].d[k]) * T.ax[2].d[l];
+        if (kind == 1) {
+            const double bx = pr.bc[0][i], by = pr.bc[1][i], bz = pr.bc[2][i];
+            acc = 0.5 * ((bx * bx + by * by) + bz * bz) * dv;
+            o.bc[0][i] += bx * dv;
+            o.bc[1][i] += by * dv;
+            o.bc[2][i] += bz * dv;
+        } else if (kind == 2) {
+            const double rho = pr.w[0][i], vx = pr.w[1][i], vy = pr.w[2][i], vz = pr.w[3][i];
+            const double vsq = (vx * vx + vy * vy) + vz * vz;
+            acc = 0.5 * rho * vsq * dv;
+            o.w[0][i] += 0.5 * vsq * dv;
+            o.w[1][i] += rho * vx * dv;
+            o.w[2][i] += rho * vy * dv;
+            o.w[3][i] += rho * vz * dv;
+        } else {
+            for (int q = 0; q < 5; ++q) acc += lamu.a[q][i] * u.a[q][i];
+            // face fields: the cell's own faces (index 1:n) plus the lower boundary faces (index 0)
+            const int st[3] = {1, b.SX, b.SX * b.SY};
+            const int own[3] = {j, k, l};
+            for (int d = 0; d < 3; ++d) {
+                acc += lamu.a[IBX + d][i] * u.a[IBX + d][i];
+                if (own[d] == 1) acc += lamu.a[IBX + d][i - st[d]] * u.a[IBX + d][i - st[d]];
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < 8; ++w) v += red[w];
+        partial[blockIdx.x] = v;
+    }
+}
+
+// clears the weights of a linear objective off its live entries
+__global__ void __launch_bounds__(256) k_adj_mask_live(Box b, Arr8 lamu) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.count()) return;
+    const int j = (int)(t % b.SX) - 2, k = (int)((t / b.SX) % b.SY) - 2, l = (int)(t / ((long long)b.SX * b.SY)) - 2;
+    const int own[3] = {j, k, l};
+    const int nn[3] = {b.nx, b.ny, b.nz};
+    const bool cell = inside(j, k, l, b);
+    for (int q = 0; q < 5; ++q)
+        if (!cell) lamu.a[q][t] = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        bool live = own[d] >= 0 && own[d] <= nn[d];
+        for (int e = 0; e < 3; ++e)
+            if (e != d && (own[e] < 1 || own[e] > nn[e])) live = false;
+        if (!live) lamu.a[IBX + d][t] = 0.0;
+    }
+}
+
+// one block: sum of n partial sums in a fixed order
+__global__ void __launch_bounds__(256) k_adj_sum(const double* partial, int n, double* out) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < 8; ++w) v += red[w];
+        *out = v;
+    }
+}
+
+}  // namespace cumc

@@ -9,6 +9,7 @@
 #include "cumc_sweep.cuh"
 #include "cumc_mixed.h"
 #include "cumc_walk.cuh"
+#include "cumc_adjoint.cuh"
 
 #include <cmath>
 #include <cstdarg>
@@ -79,6 +80,7 @@ struct cumc_ctx {
     bool mixed = false;         // CUMC_MIXED: state and kernels of cumc_mixed.cu
     MixedBufs mb{};
     MixedParams mp{};
+    double* const* tape = nullptr;  // adjoint: 3 x 8 arrays receiving each stage's combine output
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];
@@ -274,12 +276,19 @@ void combine_model(cumc_ctx* c, const Box& b, int stage, const Prim& pr, const F
     }
 }
 
-void utop(cumc_ctx* c, const Box& b, double* const* u, bool from_cons) {
+// primitive buffers of one state: the context's own, or an adjoint scratch set
+struct PrimBufs {
+    double* const* w;
+    double* const* bc;
+    double* eps;
+};
+
+void utop_into(cumc_ctx* c, const Box& b, double* const* u, const PrimBufs& p, bool from_cons) {
     UtopArgs a;
     for (int q = 0; q < 8; ++q) a.u[q] = u[q];
-    for (int q = 0; q < 5; ++q) a.w[q] = c->w[q];
-    for (int q = 0; q < 3; ++q) a.bc[q] = c->bc[q];
-    a.eps = c->eps;
+    for (int q = 0; q < 5; ++q) a.w[q] = p.w[q];
+    for (int q = 0; q < 3; ++q) a.bc[q] = p.bc[q];
+    a.eps = p.eps;
     a.ggas = c->ggas;
     a.rho_floor = c->cfg.rho_floor;
     a.eps_floor = c->cfg.eps_floor;
@@ -297,23 +306,36 @@ void utop(cumc_ctx* c, const Box& b, double* const* u, bool from_cons) {
 #undef CUMC_UTOP
 }
 
-void boundary(cumc_ctx* c, const Box& b, double* const* u) {
+void utop(cumc_ctx* c, const Box& b, double* const* u, bool from_cons) {
+    utop_into(c, b, u, PrimBufs{c->w, c->bc, c->eps}, from_cons);
+}
+
+BoundArgs bound_args(cumc_ctx* c, double* const* u, const PrimBufs& p) {
     BoundArgs a;
-    for (int q = 0; q < 5; ++q) a.w[q] = c->w[q];
-    for (int q = 0; q < 3; ++q) a.bc[q] = c->bc[q];
-    a.eps = c->eps;
+    for (int q = 0; q < 5; ++q) a.w[q] = p.w[q];
+    for (int q = 0; q < 3; ++q) a.bc[q] = p.bc[q];
+    a.eps = p.eps;
     for (int q = 0; q < 3; ++q) a.bf[q] = u[IBX + q];
     for (int q = 0; q < 6; ++q) a.flag[q] = c->flag[q];
     a.eps_yout = c->flag[2] == 0 ? 0 : c->flag[3];
     std::memcpy(a.fac, c->fac, sizeof a.fac);
     a.ggas = c->ggas;
-    const long long n = 6LL * b.SX * b.SY + 6LL * b.SX * b.nz + 6LL * b.ny * b.nz;
+    return a;
+}
+
+long long ghost_count(const Box& b) { return 6LL * b.SX * b.SY + 6LL * b.SX * b.nz + 6LL * b.ny * b.nz; }
+
+void boundary_into(cumc_ctx* c, const Box& b, double* const* u, const PrimBufs& p) {
+    const BoundArgs a = bound_args(c, u, p);
+    const long long n = ghost_count(b);
     switch (c->model) {
         case CUMC_MODEL_TORUS_SPH: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<2, double>, b, a); break;
         case CUMC_MODEL_TORUS_CYN: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<3, double>, b, a); break;
         default: launch(c, CUMC_K_BOUNDARY, n, 256, k_boundary<0, double>, b, a); break;
     }
 }
+
+void boundary(cumc_ctx* c, const Box& b, double* const* u) { boundary_into(c, b, u, PrimBufs{c->w, c->bc, c->eps}); }
 
 Prim make_prim(cumc_ctx* c, double* const* u) {
     Prim p;
@@ -381,6 +403,11 @@ void run_stage(cumc_ctx* c, const Box& b, int stage) {
         default: combine_model<3>(c, b, stage, pr, ff, a); break;
     }
     if (stage == 0) return;
+    if (c->tape) {  // adjoint recomputation: keep the combine's output of this stage
+        const size_t bytes = (size_t)b.count() * sizeof(double);
+        for (int q = 0; q < 8; ++q)
+            cudaMemcpyAsync(c->tape[(stage - 1) * 8 + q], dst[q], bytes, cudaMemcpyDeviceToDevice, c->stream);
+    }
     utop(c, b, dst, true);
     boundary(c, b, dst);
 }
@@ -959,3 +986,303 @@ int cumc_launch_count(cumc_ctx* c, long long* count) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// discrete adjoint (cumc_adjoint_run): checkpointed forward pass, then per
+// segment a recomputation that tapes each stage's combine output, then the
+// reverse sweep of the kernels in cumc_adjoint.cuh
+// ---------------------------------------------------------------------------
+namespace {
+
+// device scratch of one adjoint run, released on every return path
+struct AdjMem {
+    std::vector<void*> v;
+    ~AdjMem() {
+        for (void* p : v) cudaFree(p);
+    }
+};
+
+int adj_alloc(cumc_ctx* c, AdjMem& m, double** p, size_t n) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return c->fail(CUMC_ERR_NOMEM, "adjoint: cudaMalloc of %zu bytes failed: %s", n * sizeof(double),
+                       cudaGetErrorString(e));
+    }
+    m.v.push_back(q);
+    *p = static_cast<double*>(q);
+    return CUMC_OK;
+}
+
+// one state: conserved U (face fields included) and primitives with ghosts
+struct StateSet {
+    double* u[8];
+    double* w[5];
+    double* bc[3];
+    double* eps;
+    PrimBufs prim() const { return PrimBufs{w, bc, eps}; }
+    Prim as_prim() const {
+        Prim p;
+        for (int q = 0; q < 5; ++q) p.w[q] = w[q];
+        for (int q = 0; q < 3; ++q) p.bc[q] = bc[q];
+        for (int q = 0; q < 3; ++q) p.bf[q] = u[IBX + q];
+        return p;
+    }
+    double** all(int i) { return i < 8 ? &u[i] : i < 13 ? &w[i - 8] : i < 16 ? &bc[i - 13] : &eps; }
+};
+constexpr int STATE_ARRAYS = 17;
+
+int adj_state(cumc_ctx* c, AdjMem& m, StateSet& s) {
+    for (int i = 0; i < STATE_ARRAYS; ++i) {
+        int rc = adj_alloc(c, m, s.all(i), (size_t)c->box.count());
+        if (rc != CUMC_OK) return rc;
+    }
+    return CUMC_OK;
+}
+
+StateSet live_state(cumc_ctx* c) {
+    StateSet s;
+    for (int q = 0; q < 8; ++q) s.u[q] = c->U[c->cur][q];
+    for (int q = 0; q < 5; ++q) s.w[q] = c->w[q];
+    for (int q = 0; q < 3; ++q) s.bc[q] = c->bc[q];
+    s.eps = c->eps;
+    return s;
+}
+
+void copy_state(cumc_ctx* c, StateSet dst, StateSet src) {
+    const size_t bytes = (size_t)c->box.count() * sizeof(double);
+    for (int i = 0; i < STATE_ARRAYS; ++i)
+        cudaMemcpyAsync(*dst.all(i), *src.all(i), bytes, cudaMemcpyDeviceToDevice, c->stream);
+}
+
+// primitives (and boundary-filled face fields) of a taped combine output
+void adj_prims_from(cumc_ctx* c, const Box& b, double* const* upre, StateSet& P) {
+    const size_t bytes = (size_t)b.count() * sizeof(double);
+    for (int q = 0; q < 8; ++q) cudaMemcpyAsync(P.u[q], upre[q], bytes, cudaMemcpyDeviceToDevice, c->stream);
+    utop_into(c, b, P.u, P.prim(), true);
+    boundary_into(c, b, P.u, P.prim());
+}
+
+Arr8 arr8(double* const* p, int n = 8) {
+    Arr8 a{};
+    for (int q = 0; q < n; ++q) a.a[q] = p[q];
+    return a;
+}
+Arr3 arr3(double* const* p) {
+    Arr3 a;
+    for (int q = 0; q < 3; ++q) a.a[q] = p[q];
+    return a;
+}
+
+template <int RECON>
+void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, const AdjPrim& lp, double* const* lbf) {
+    const long long nx = (long long)(b.nx + 1) * (b.ny + 2) * (b.nz + 2);
+    const long long ny = (long long)(b.nx + 2) * (b.ny + 1) * (b.nz + 2);
+    const long long nz = (long long)(b.nx + 2) * (b.ny + 2) * (b.nz + 1);
+    launch(c, -1, nx, 128, k_adj_sweep<0, RECON>, b, c->tabs, pr, c->ggas, st, lp, lbf[0]);
+    launch(c, -1, ny, 128, k_adj_sweep<1, RECON>, b, c->tabs, pr, c->ggas, st, lp, lbf[1]);
+    launch(c, -1, nz, 128, k_adj_sweep<2, RECON>, b, c->tabs, pr, c->ggas, st, lp, lbf[2]);
+}
+
+template <bool FROM_CONS>
+void adj_utop(cumc_ctx* c, const Box& b, Arr8 u, Arr8 w0, const double* eps0, Arr8 lu, const AdjPrim& lp, Arr8 mu,
+              Arr3 lb) {
+    const long long n = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
+    if (c->model == CUMC_MODEL_RIEMANN)
+        launch(c, -1, n, 256, k_adj_utop<1, FROM_CONS>, b, u, w0, eps0, lu, lp, c->ggas, mu, lb);
+    else
+        launch(c, -1, n, 256, k_adj_utop<0, FROM_CONS>, b, u, w0, eps0, lu, lp, c->ggas, mu, lb);
+}
+
+int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const double* dt_in, double* dt_out,
+                double* J, double* grad_prim, double* grad_eps) {
+    const Box b = c->box;
+    const size_t NT = (size_t)b.count();
+    const size_t bytes = NT * sizeof(double);
+    const int nck = (N + K - 1) / K;
+    const size_t arrays = (size_t)nck * STATE_ARRAYS + (size_t)K * 24 + 3 * STATE_ARRAYS + 8 * 3 + 3 * 2 + 9;
+    {
+        size_t fr = 0, tot = 0;
+        CUMC_CHECK(cudaMemGetInfo(&fr, &tot));
+        if (arrays * bytes + (256u << 20) > fr)
+            return c->fail(CUMC_ERR_NOMEM, "adjoint needs %.2f GB of device memory (%zu arrays), %.2f GB free",
+                           arrays * bytes / 1e9, arrays, fr / 1e9);
+    }
+    AdjMem m;
+    int rc;
+    std::vector<StateSet> ck(nck);
+    for (auto& s : ck)
+        if ((rc = adj_state(c, m, s)) != CUMC_OK) return rc;
+    std::vector<double*> tape((size_t)K * 24);
+    for (auto& p : tape)
+        if ((rc = adj_alloc(c, m, &p, NT)) != CUMC_OK) return rc;
+    StateSet P[2], fin;
+    for (StateSet* s : {&P[0], &P[1], &fin})
+        if ((rc = adj_state(c, m, *s)) != CUMC_OK) return rc;
+    double *lamA[8], *lamB[8], *mu[8], *lb[3], *lamE[3];
+    AdjPrim lp;
+    for (double** p : {lamA, lamB, mu})
+        for (int q = 0; q < 8; ++q)
+            if ((rc = adj_alloc(c, m, &p[q], NT)) != CUMC_OK) return rc;
+    for (double** p : {lb, lamE})
+        for (int q = 0; q < 3; ++q)
+            if ((rc = adj_alloc(c, m, &p[q], NT)) != CUMC_OK) return rc;
+    for (int q = 0; q < 5; ++q)
+        if ((rc = adj_alloc(c, m, &lp.w[q], NT)) != CUMC_OK) return rc;
+    for (int q = 0; q < 3; ++q)
+        if ((rc = adj_alloc(c, m, &lp.bc[q], NT)) != CUMC_OK) return rc;
+    if ((rc = adj_alloc(c, m, &lp.eps, NT)) != CUMC_OK) return rc;
+    const long long ncell = (long long)b.nx * b.ny * b.nz;
+    const int nblk = (int)((ncell + 255) / 256);
+    double *partial, *ddt;
+    if ((rc = adj_alloc(c, m, &partial, (size_t)nblk + 1)) != CUMC_OK) return rc;
+    if ((rc = adj_alloc(c, m, &ddt, (size_t)N)) != CUMC_OK) return rc;
+    auto zero = [&](double* p) { cudaMemsetAsync(p, 0, bytes, c->stream); };
+    for (double** p : {lamA, lamB, mu})
+        for (int q = 0; q < 8; ++q) zero(p[q]);
+    for (int q = 0; q < 3; ++q) { zero(lb[q]); zero(lamE[q]); }
+    auto zero_lp = [&]() {
+        for (int q = 0; q < 5; ++q) zero(lp.w[q]);
+        for (int q = 0; q < 3; ++q) zero(lp.bc[q]);
+        zero(lp.eps);
+    };
+    zero_lp();
+
+    // ---- forward pass with checkpoints (initial_update, then N steps) ------
+    utop(c, b, c->U[c->cur], false);
+    boundary(c, b, c->U[c->cur]);
+    std::vector<double> dts((size_t)N);
+    for (int n = 0; n < N; ++n) {
+        if (n % K == 0) copy_state(c, ck[n / K], live_state(c));
+        double dt;
+        if (dt_in) {
+            dt = dt_in[n];
+        } else {
+            finddt_launch(c, b);
+            CUMC_CHECK(cudaMemcpyAsync(c->host_pinned, c->dtmin, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+            CUMC_CHECK(cudaStreamSynchronize(c->stream));
+            std::memcpy(&dt, c->host_pinned, sizeof(double));
+        }
+        dts[n] = dt;
+        launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
+        rk_step(c, b);
+    }
+    copy_state(c, fin, live_state(c));
+    CUMC_CHECK(cudaMemcpyAsync(c->host_pinned + 1, c->flag_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    if ((rc = sync_status(c)) != CUMC_OK) return rc;
+    {
+        unsigned fl;
+        std::memcpy(&fl, c->host_pinned + 1, sizeof(unsigned));
+        if (fl & 1u) return c->fail(CUMC_ERR_NONFINITE, "adjoint: non-finite state in the forward pass");
+    }
+    CUMC_CHECK(cudaMemcpyAsync(ddt, dts.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+
+    // ---- objective and seed --------------------------------------------------
+    double** lamCur = lamA;  // adjoint of the state at the current stage boundary
+    double** lamU0 = lamB;   // adjoint of the step's starting state (accumulated)
+    if (obj == CUMC_OBJ_LINEAR) {
+        if ((rc = put_soa(c, weights, 8, lamCur)) != CUMC_OK) return rc;
+        launch(c, -1, (long long)NT, 256, k_adj_mask_live, b, arr8(lamCur));
+    }
+    launch(c, -1, ncell, 256, k_adj_objective, b, c->tabs, fin.as_prim(), arr8(fin.u), obj, lp, arr8(lamCur), partial);
+    launch(c, -1, 256, 256, k_adj_sum, (const double*)partial, nblk, partial + nblk);
+    CUMC_CHECK(cudaMemcpyAsync(c->host_pinned, partial + nblk, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    if (J) std::memcpy(J, c->host_pinned, sizeof(double));
+
+    // ---- reverse sweep -----------------------------------------------------
+    constexpr double alpha[4] = {0.0, 1.0, 3.0 / 4.0, 1.0 / 3.0};
+    constexpr double beta[4] = {0.0, 0.0, 1.0 / 4.0, 2.0 / 3.0};
+    constexpr double gam[4] = {0.0, 1.0, 1.0 / 4.0, 2.0 / 3.0};
+    int pc = 0;
+    bool have_next = false;  // P[pc] holds the primitives after step n
+    for (int seg = nck - 1; seg >= 0; --seg) {
+        const int a0 = seg * K, a1 = std::min(N, a0 + K);
+        copy_state(c, live_state(c), ck[seg]);
+        for (int n = a0; n < a1; ++n) {
+            c->tape = &tape[(size_t)(n - a0) * 24];
+            launch(c, -1, 1, 1, k_set_scalar, c->scal, dts[n]);
+            rk_step(c, b);
+        }
+        c->tape = nullptr;
+        for (int n = a1 - 1; n >= a0; --n) {
+            double* const* tp = &tape[(size_t)(n - a0) * 24];
+            if (!have_next) adj_prims_from(c, b, tp + 16, P[pc]);
+            for (int q = 0; q < 8; ++q) zero(lamU0[q]);
+            for (int s = 3; s >= 1; --s) {
+                StateSet& Pc = P[pc];
+                StateSet& Pp = P[1 - pc];
+                if (s >= 2) adj_prims_from(c, b, tp + (s - 2) * 8, Pp);
+                else if (n > a0) adj_prims_from(c, b, &tape[(size_t)(n - 1 - a0) * 24 + 16], Pp);
+                else copy_state(c, Pp, ck[seg]);
+                // boundary^T and utop^T of the stage's output
+                launch(c, -1, ghost_count(b), 256, k_adj_boundary, b, bound_args(c, Pc.u, Pc.prim()), lp,
+                       lamCur[IBX], lamCur[IBY], lamCur[IBZ]);
+                adj_utop<true>(c, b, arr8(tp + (s - 1) * 8), arr8(Pc.w, 5), nullptr, arr8(lamCur), lp, arr8(mu), arr3(lb));
+                launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_bface, b, arr3(lamCur + IBX),
+                       arr3(lb), arr3(mu + IBX));
+                // combine^T
+                launch(c, -1, (long long)NT, 256, k_adj_combine, (long long)NT, arr8(mu), alpha[s], beta[s],
+                       arr8(lamU0), arr8(lamCur));
+                zero_lp();
+                // L^T at the stage's input
+                AdjStage st;
+                for (int q = 0; q < 8; ++q) st.mu[q] = mu[q];
+                for (int q = 0; q < 3; ++q) st.lamE[q] = lamE[q];
+                st.dt = ddt + n;
+                st.gam = gam[s];
+                launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_ct, b, c->tabs, st,
+                       lamE[0], lamE[1], lamE[2]);
+                const Prim pr = Pp.as_prim();
+                launch(c, -1, (long long)(b.nx + 2) * (b.ny + 2) * (b.nz + 2), 256, k_adj_ecell, b, pr,
+                       (const double*)lamE[0], (const double*)lamE[1], (const double*)lamE[2], lp);
+                double* const* lbf = s >= 2 ? lamCur + IBX : lamU0 + IBX;
+                if (c->recon == CUMC_PPMC) adj_sweeps<4>(c, b, pr, st, lp, lbf);
+                else adj_sweeps<1>(c, b, pr, st, lp, lbf);
+                pc = 1 - pc;
+            }
+            std::swap(lamCur, lamU0);  // adjoint of the step's starting state
+            have_next = true;
+        }
+    }
+    // ---- initial_update^T: P[pc] and ck[0] hold the state after initial_update
+    launch(c, -1, ghost_count(b), 256, k_adj_boundary, b, bound_args(c, ck[0].u, ck[0].prim()), lp, lamCur[IBX],
+           lamCur[IBY], lamCur[IBZ]);
+    adj_utop<false>(c, b, arr8(ck[0].u), arr8(ck[0].w, 5), ck[0].eps, arr8(lamCur), lp, arr8(mu), arr3(lb));
+    launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_bface, b, arr3(lamCur + IBX), arr3(lb),
+           arr3(mu + IBX));
+    if ((rc = sync_status(c)) != CUMC_OK) return rc;
+    if (grad_prim) {
+        const double* s[8] = {mu[0], mu[1], mu[2], mu[3], nullptr, mu[IBX], mu[IBY], mu[IBZ]};
+        if ((rc = get_soa(c, grad_prim, 8, s)) != CUMC_OK) return rc;
+    }
+    if (grad_eps) {
+        const double* s[1] = {mu[4]};
+        if ((rc = get_soa(c, grad_eps, 1, s)) != CUMC_OK) return rc;
+    }
+    if (dt_out) std::memcpy(dt_out, dts.data(), (size_t)N * sizeof(double));
+    copy_state(c, live_state(c), fin);
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    c->ready = true;
+    return sync_status(c);
+}
+
+}  // namespace
+
+extern "C" int cumc_adjoint_run(cumc_ctx* c, int nsteps, int checkpoint_every, int objective, const double* weights,
+                                const double* dt_in, double* dt_out, double* J, double* grad_prim, double* grad_eps) {
+    if (!c) return CUMC_ERR_ARG;
+    if (!c->uploaded) return c->fail(CUMC_ERR_STATE, "cumc_upload_state must come first");
+    if (c->mixed || c->coord != CUMC_CARTESIAN ||
+        (c->model != CUMC_MODEL_NONE && c->model != CUMC_MODEL_RIEMANN))
+        return c->fail(CUMC_ERR_CONFIG, "the adjoint covers CUMC_FP64 on CUMC_CARTESIAN grids with model NONE or RIEMANN");
+    if (nsteps < 1 || checkpoint_every < 1) return c->fail(CUMC_ERR_ARG, "nsteps and checkpoint_every must be >= 1");
+    if (objective < CUMC_OBJ_MAGNETIC || objective > CUMC_OBJ_LINEAR) return c->fail(CUMC_ERR_ARG, "unknown objective");
+    if (objective == CUMC_OBJ_LINEAR && !weights) return c->fail(CUMC_ERR_ARG, "CUMC_OBJ_LINEAR needs weights");
+    const int rc = adjoint_run(c, nsteps, std::min(checkpoint_every, nsteps), objective, weights, dt_in, dt_out, J,
+                               grad_prim, grad_eps);
+    c->tape = nullptr;
+    return rc;
+}

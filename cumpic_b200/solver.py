@@ -128,6 +128,28 @@ class CUMC3D:
         """`nsteps` iterations of the main loop on the device (no host sync between)."""
         return self.run(total_time, nsteps)
 
+    # -- discrete adjoint ------------------------------------------------------
+    def adjoint(self, nsteps: int, checkpoint_every: int = 20, objective: int = N.OBJ_MAGNETIC,
+                weights: np.ndarray | None = None, dts: np.ndarray | None = None) -> dict:
+        """cumc_adjoint_run: from the uploaded state, initial_update and
+        `nsteps` steps (dt from `dts` when given, else finddt), then the
+        objective J on the final state and its gradient with respect to the
+        uploaded prim (rho, v, face B; the pressure slot is 0) and eps.
+        Returns {"J", "grad_prim", "grad_eps", "dts"}; the context then holds
+        the final state."""
+        gp = np.zeros(self.shape + (8,))
+        ge = np.zeros(self.shape)
+        dt_out = np.zeros(nsteps)
+        J = ctypes.c_double()
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        d_in = None if dts is None else np.ascontiguousarray(dts, dtype=np.float64)
+        self._check(self._lib.cumc_adjoint_run(self._h, int(nsteps), int(checkpoint_every), int(objective),
+                                               None if w is None else _dp(w), None if d_in is None else _dp(d_in),
+                                               _dp(dt_out), ctypes.byref(J), _dp(gp), _dp(ge)))
+        self.n_step = nsteps
+        self.global_time = float(np.sum(dt_out))
+        return {"J": J.value, "grad_prim": gp, "grad_eps": ge, "dts": dt_out}
+
     # -- instrumentation -----------------------------------------------------
     def stream_handle(self) -> int:
         s = ctypes.c_void_p()

@@ -175,6 +175,45 @@ int cumc_profile_read(cumc_ctx* ctx, int which, int* launches, double* ms);
 /* Number of kernel launches the library issued since cumc_init. */
 int cumc_launch_count(cumc_ctx* ctx, long long* count);
 
+/* Discrete adjoint of the FP64 path. No counterpart in the reference, which
+ * has no derivatives; it is the new entry point cumc_adjoint_run of the hot
+ * path's drop-in boundary.
+ *
+ * Starting from the state last given to cumc_upload_state, runs
+ * initial_update and nsteps RUNGEKUTTA steps, evaluates the objective J on
+ * the final state and returns dJ/d(uploaded state) by the transpose of every
+ * kernel of the step (reconstruction limiters, extremum fixes and HLL wave
+ * choices frozen as the forward pass took them; HLL, CT, boundaries and the
+ * conversions differentiated exactly). The dt sequence is frozen: taken from
+ * dt_in[0..nsteps) when given, else from finddt each step, and returned in
+ * dt_out (may be NULL). Memory is traded for recomputation: the forward state
+ * is checkpointed every checkpoint_every steps and each segment is recomputed
+ * once during the reverse sweep; this needs
+ *   (ceil(nsteps/checkpoint_every) * 17 + checkpoint_every * 24 + 93)
+ * arrays of (nx+6)(ny+6)(nz+6) doubles of device memory (CUMC_ERR_NOMEM if
+ * absent).
+ *
+ * objective: CUMC_OBJ_MAGNETIC  J = 1/2 sum |bcell|^2 dV over the active cells
+ *            CUMC_OBJ_KINETIC   J = 1/2 sum rho |v|^2 dV
+ *            CUMC_OBJ_LINEAR    J = sum weights . cons over the entries the
+ *                               step defines (active cells; face fields at
+ *                               index 0:n along their axis, 1:n across);
+ *                               weights in the cons layout.
+ * grad_prim (prim layout, may be NULL): dJ/d(rho, vx, vy, vz) in slots 1-4,
+ *            0 in slot 5 (initial_update takes the pressure from eps), and
+ *            dJ/d(face Bx, By, Bz) in slots 6-8; grad_eps (eps layout, may be
+ *            NULL): dJ/d(eps). Ghost entries, which initial_update
+ *            overwrites, get 0.
+ * On return the context holds the final state, as after cumc_initial_update
+ * and nsteps cumc_rungekutta calls. Supported: CUMC_FP64, CUMC_CARTESIAN,
+ * models NONE and RIEMANN (CUMC_ERR_CONFIG otherwise). */
+#define CUMC_OBJ_MAGNETIC 1
+#define CUMC_OBJ_KINETIC  2
+#define CUMC_OBJ_LINEAR   3
+int cumc_adjoint_run(cumc_ctx* ctx, int nsteps, int checkpoint_every, int objective,
+                     const double* weights, const double* dt_in, double* dt_out,
+                     double* J, double* grad_prim, double* grad_eps);
+
 /* CFL time step over caller-owned device arrays, allocating nothing.
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory when they need a time step, such as a code capturing

@@ -56,8 +56,47 @@ inline double MIN2(double a, double b) { return std::fmin(a, b); }
 inline double MAX2(double a, double b) { return std::fmax(a, b); }
 inline double MIN3(double a, double b, double c) { return std::fmin(std::fmin(a, b), c); }
 inline double MAX3(double a, double b, double c) { return std::fmax(std::fmax(a, b), c); }
+inline double sqrt_(double a) { return std::sqrt(a); }
+inline double fabs_(double a) { return std::fabs(a); }
+inline double val(double a) { return a; }
 
-struct Oracle {
+// Tangent-linear scalar: a value and one directional derivative. Values are
+// computed with exactly the double operations above, so a Dual run follows
+// the same branches as the double run on the same inputs (limiter, extremum
+// and HLL choices frozen at the base point) and its derivative parts are the
+// exact directional derivative of the discrete map.
+struct Dual {
+    double v, d;
+    Dual() : v(0.0), d(0.0) {}
+    Dual(double x) : v(x), d(0.0) {}  // constants carry no derivative
+    Dual(double x, double t) : v(x), d(t) {}
+};
+inline Dual operator+(const Dual& a, const Dual& b) { return Dual(a.v + b.v, a.d + b.d); }
+inline Dual operator-(const Dual& a, const Dual& b) { return Dual(a.v - b.v, a.d - b.d); }
+inline Dual operator-(const Dual& a) { return Dual(-a.v, -a.d); }
+inline Dual operator*(const Dual& a, const Dual& b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+inline Dual operator/(const Dual& a, const Dual& b) {
+    const double q = a.v / b.v;
+    return Dual(q, (a.d - q * b.d) / b.v);
+}
+inline bool operator<(const Dual& a, const Dual& b) { return a.v < b.v; }
+inline bool operator>(const Dual& a, const Dual& b) { return a.v > b.v; }
+inline bool operator<=(const Dual& a, const Dual& b) { return a.v <= b.v; }
+inline bool operator>=(const Dual& a, const Dual& b) { return a.v >= b.v; }
+inline double SIGN1(const Dual& b) { return std::copysign(1.0, b.v); }
+inline Dual MIN2(const Dual& a, const Dual& b) { return b.v < a.v ? b : a; }
+inline Dual MAX2(const Dual& a, const Dual& b) { return b.v > a.v ? b : a; }
+inline Dual MIN3(const Dual& a, const Dual& b, const Dual& c) { return MIN2(MIN2(a, b), c); }
+inline Dual MAX3(const Dual& a, const Dual& b, const Dual& c) { return MAX2(MAX2(a, b), c); }
+inline Dual sqrt_(const Dual& a) {
+    const double s = std::sqrt(a.v);
+    return Dual(s, s > 0.0 ? a.d / (2.0 * s) : 0.0);
+}
+inline Dual fabs_(const Dual& a) { return a.v < 0.0 ? -a : a; }
+inline double val(const Dual& a) { return a.v; }
+
+template <typename T>
+struct OracleT {
     cumc_config cfg{};
     int nx = 0, ny = 0, nz = 0;
     size_t SX = 0, SY = 0, SZ = 0, NT = 0;
@@ -71,22 +110,22 @@ struct Oracle {
     int geom_repeat = 8;
 
     std::vector<double> xF, yF, zF;  // index -3..n+3 stored at [i+3]
-    std::vector<double> prim, cons, primL, primR, consL, consR, fluxL, fluxR, flux;
-    std::vector<double> l_rk, u_old, sc, bcell, ecell, ecorn, eps;
+    std::vector<T> prim, cons, primL, primR, consL, consR, fluxL, fluxR, flux;
+    std::vector<T> l_rk, u_old, sc, bcell, ecell, ecorn, eps;
     double dt = 0;
 
     // ---- indexing (Fortran column-major, lower bound -2 on space) ----
     inline size_t ix(int j, int k, int l) const {
         return (size_t)(j + 2) + SX * ((size_t)(k + 2) + SY * (size_t)(l + 2));
     }
-    inline double& A8(std::vector<double>& a, int i, int j, int k, int l) {
+    inline T& A8(std::vector<T>& a, int i, int j, int k, int l) {
         return a[(size_t)(i - 1) + 8 * ix(j, k, l)];
     }
-    inline double& B3(int i, int j, int k, int l) { return bcell[(size_t)(i - ibx) + 3 * ix(j, k, l)]; }
-    inline double& E3(std::vector<double>& a, int i, int j, int k, int l) {
+    inline T& B3(int i, int j, int k, int l) { return bcell[(size_t)(i - ibx) + 3 * ix(j, k, l)]; }
+    inline T& E3(std::vector<T>& a, int i, int j, int k, int l) {
         return a[(size_t)(i - 1) + 3 * ix(j, k, l)];
     }
-    inline double& EPS(int j, int k, int l) { return eps[ix(j, k, l)]; }
+    inline T& EPS(int j, int k, int l) { return eps[ix(j, k, l)]; }
     inline double XF(int j) const { return xF[(size_t)(j + 3)]; }
     inline double YF(int k) const { return yF[(size_t)(k + 3)]; }
     inline double ZF(int l) const { return zF[(size_t)(l + 3)]; }
@@ -110,16 +149,16 @@ struct Oracle {
         double x, y, z, dxl, dyl, dzl;
         get_coord(j, k, l, x, y, z);
         coord_dx(j, k, l, dxl, dyl, dzl);
-        const double bx = B3(ibx, j, k, l), by = B3(iby, j, k, l), bz = B3(ibz, j, k, l);
-        const double rho = A8(prim, irho, j, k, l), vx = A8(prim, ivx, j, k, l);
-        const double vy = A8(prim, ivy, j, k, l), vz = A8(prim, ivz, j, k, l);
-        const double p = A8(prim, itau, j, k, l);
+        const T bx = B3(ibx, j, k, l), by = B3(iby, j, k, l), bz = B3(ibz, j, k, l);
+        const T rho = A8(prim, irho, j, k, l), vx = A8(prim, ivx, j, k, l);
+        const T vy = A8(prim, ivy, j, k, l), vz = A8(prim, ivz, j, k, l);
+        const T p = A8(prim, itau, j, k, l);
         if (coordinate == CUMC_CYLINDRICAL) {
-            const double bsquare = bx * bx + by * by + bz * bz;
+            const T bsquare = bx * bx + by * by + bz * bz;
             A8(sc, ivx, j, k, l) = A8(sc, ivx, j, k, l) + (((p + (rho * vy) * vy) + 0.5 * bsquare) - by * by) / (x);
             A8(sc, ivy, j, k, l) = A8(sc, ivy, j, k, l) - ((rho * vx) * vy - bx * by) / (x);
         } else if (coordinate == CUMC_SPHERICAL) {
-            const double bsquare = bx * bx + by * by + bz * bz;
+            const T bsquare = bx * bx + by * by + bz * bz;
             const double tany = std::tan(y);
             A8(sc, ivx, j, k, l) = A8(sc, ivx, j, k, l) + ((2.0 * p + bx * bx) + rho * (vy * vy + vz * vz)) / (x);
             A8(sc, ivy, j, k, l) = (A8(sc, ivy, j, k, l) + (((p + (rho * vz) * vz) + 0.5 * bsquare) - bz * bz) / (x * tany))
@@ -222,9 +261,9 @@ struct Oracle {
     }
 
     // ---- EOS (model/riemann/src/eos.f90:126-200) ----
-    inline double eos_pressure(double rho, double e) const { return (rho * e) * (ggas - 1.0); }
-    inline double eos_soundspeed(double p, double rho) const { return std::sqrt((ggas * p) / rho); }
-    inline double eos_epsilon(double p, double rho) const { return (p / rho) / (ggas - 1.0); }
+    inline T eos_pressure(const T& rho, const T& e) const { return (rho * e) * (ggas - 1.0); }
+    inline T eos_soundspeed(const T& p, const T& rho) const { return sqrt_((ggas * p) / rho); }
+    inline T eos_epsilon(const T& p, const T& rho) const { return (p / rho) / (ggas - 1.0); }
 
     // ---- reconstruction (solver/reconstruct.f90) ----
     void dh3(int dir, int j, int k, int l, int off, double& d) const {
@@ -235,8 +274,7 @@ struct Oracle {
     }
 
     // TVD_MM (solver/reconstruct.f90:58-128)
-    void tvd_mm(int dir, int j, int k, int l, double vm2, double vm1, double vc, double vp1, double vp2,
-                double& vm_out, double& vp_out) const {
+    void tvd_mm(int dir, int j, int k, int l, T vm2, T vm1, T vc, T vp1, T vp2, T& vm_out, T& vp_out) const {
         (void)vm2; (void)vp2;
         double dh_m1, dh_c, dh_p1;
         dh3(dir, j, k, l, -1, dh_m1);
@@ -244,16 +282,15 @@ struct Oracle {
         dh3(dir, j, k, l, 1, dh_p1);
         const double cf = (dh_c + dh_p1) / dh_c;
         const double cb = (dh_c + dh_m1) / dh_c;
-        const double dqf = (2.0 * (vp1 - vc)) / cf;
-        const double dqb = (2.0 * (vc - vm1)) / cb;
-        const double slope = (0.5 * (SIGN1(dqf) + SIGN1(dqb))) * MIN2(std::fabs(dqf), std::fabs(dqb));
+        const T dqf = (2.0 * (vp1 - vc)) / cf;
+        const T dqb = (2.0 * (vc - vm1)) / cb;
+        const T slope = (0.5 * (SIGN1(dqf) + SIGN1(dqb))) * MIN2(fabs_(dqf), fabs_(dqb));
         vp_out = vc + 0.5 * slope;
         vm_out = vc - 0.5 * slope;
     }
 
     // PPM (solver/reconstruct.f90:137-311)
-    void ppm(int dir, int j, int k, int l, double vm2, double vm1, double vc, double vp1, double vp2,
-             double& vm_out, double& vp_out) const {
+    void ppm(int dir, int j, int k, int l, T vm2, T vm1, T vc, T vp1, T vp2, T& vm_out, T& vp_out) const {
         double dm2, dm1, dc, dp1, dp2;
         dh3(dir, j, k, l, -2, dm2);
         dh3(dir, j, k, l, -1, dm1);
@@ -293,27 +330,27 @@ struct Oracle {
         const double b0c = cc1 * cc2, b1c = cc1 * cc3;
         const double b0p = cp1 * cp2, b1p = cp1 * cp3;
         // :254-256
-        const double deltap1 = b0p * (vp2 - vp1) + b1p * (vp1 - vc);
-        const double deltac = b0c * (vp1 - vc) + b1c * (vc - vm1);
-        const double deltam1 = b0m * (vc - vm1) + b1m * (vm1 - vm2);
+        const T deltap1 = b0p * (vp2 - vp1) + b1p * (vp1 - vc);
+        const T deltac = b0c * (vp1 - vc) + b1c * (vc - vm1);
+        const T deltam1 = b0m * (vc - vm1) + b1m * (vm1 - vm2);
         // :261-280 van Leer limiter
-        double dmc, dmp1, dmm1;
+        T dmc, dmp1, dmm1;
         if ((vp1 - vc) * (vc - vm1) > 0.0)
-            dmc = MIN3(std::fabs(deltac), 2.0 * std::fabs(vc - vm1), 2.0 * std::fabs(vc - vp1)) * SIGN1(deltac);
+            dmc = MIN3(fabs_(deltac), 2.0 * fabs_(vc - vm1), 2.0 * fabs_(vc - vp1)) * SIGN1(deltac);
         else
             dmc = 0.0;
         if ((vp2 - vp1) * (vp1 - vc) > 0.0)
-            dmp1 = MIN3(std::fabs(deltap1), 2.0 * std::fabs(vp1 - vc), 2.0 * std::fabs(vp1 - vp2)) * SIGN1(deltap1);
+            dmp1 = MIN3(fabs_(deltap1), 2.0 * fabs_(vp1 - vc), 2.0 * fabs_(vp1 - vp2)) * SIGN1(deltap1);
         else
             dmp1 = 0.0;
         if ((vc - vm1) * (vm1 - vm2) > 0.0)
-            dmm1 = MIN3(std::fabs(deltam1), 2.0 * std::fabs(vm1 - vm2), 2.0 * std::fabs(vm1 - vc)) * SIGN1(deltam1);
+            dmm1 = MIN3(fabs_(deltam1), 2.0 * fabs_(vm1 - vm2), 2.0 * fabs_(vm1 - vc)) * SIGN1(deltam1);
         else
             dmm1 = 0.0;
         // :285-286
         vp_out = (((vc + a0p * (vp1 - vc)) + a1p * (vp1 - vc)) + a2p * dmp1) + a3p * dmc;
         vm_out = (((vm1 + a0m * (vc - vm1)) + a1m * (vc - vm1)) + a2m * dmc) + a3m * dmm1;
-        const double vl = vm_out, vr = vp_out;
+        const T vl = vm_out, vr = vp_out;
         // :295-307 extremum and overshoot fixes; the second test reads the
         // already-modified vm_out
         if ((vr - vc) * (vc - vl) <= 0.0) {
@@ -326,20 +363,19 @@ struct Oracle {
     }
 
     // INTERPOLATE (solver/reconstruct.f90:18-51)
-    void interpolate(int dir, int j, int k, int l, double vm2, double vm1, double vc, double vp1, double vp2,
-                     double& vm_out, double& vp_out) const {
+    void interpolate(int dir, int j, int k, int l, T vm2, T vm1, T vc, T vp1, T vp2, T& vm_out, T& vp_out) const {
         if (recon == CUMC_TVDMM) tvd_mm(dir, j, k, l, vm2, vm1, vc, vp1, vp2, vm_out, vp_out);
         else ppm(dir, j, k, l, vm2, vm1, vc, vp1, vp2, vm_out, vp_out);
     }
 
     // ---- Riemann solver (solver/rsolver.f90, flux.f90, ptou_face.f90) ----
     // PtoU_MHD_face (solver/ptou_face.f90:34-88)
-    void ptou_face(std::vector<double>& P, std::vector<double>& U, int j, int k, int l, double e) {
-        const double vx = A8(P, ivx, j, k, l), vy = A8(P, ivy, j, k, l), vz = A8(P, ivz, j, k, l);
-        const double bx = A8(P, ibx, j, k, l), by = A8(P, iby, j, k, l), bz = A8(P, ibz, j, k, l);
-        const double rho = A8(P, irho, j, k, l);
-        const double vsquare = (vx * vx + vy * vy) + vz * vz;
-        const double bsquare = (bx * bx + by * by) + bz * bz;
+    void ptou_face(std::vector<T>& P, std::vector<T>& U, int j, int k, int l, const T& e) {
+        const T vx = A8(P, ivx, j, k, l), vy = A8(P, ivy, j, k, l), vz = A8(P, ivz, j, k, l);
+        const T bx = A8(P, ibx, j, k, l), by = A8(P, iby, j, k, l), bz = A8(P, ibz, j, k, l);
+        const T rho = A8(P, irho, j, k, l);
+        const T vsquare = (vx * vx + vy * vy) + vz * vz;
+        const T bsquare = (bx * bx + by * by) + bz * bz;
         A8(U, irho, j, k, l) = rho;
         A8(U, ivx, j, k, l) = vx * rho;
         A8(U, ivy, j, k, l) = vy * rho;
@@ -351,18 +387,17 @@ struct Oracle {
     }
 
     // Ptof_MHD, one side (solver/flux.f90:163-262)
-    void ptof_side(std::vector<double>& P, std::vector<double>& U, std::vector<double>& F, int dir, int j,
-                   int k, int l) {
+    void ptof_side(std::vector<T>& P, std::vector<T>& U, std::vector<T>& F, int dir, int j, int k, int l) {
         int ivn, ivt1, ivt2, ibn, ibt1, ibt2;
         if (dir == x_dir) { ivn = ivx; ivt1 = ivy; ivt2 = ivz; ibn = ibx; ibt1 = iby; ibt2 = ibz; }
         else if (dir == y_dir) { ivn = ivy; ivt1 = ivz; ivt2 = ivx; ibn = iby; ibt1 = ibz; ibt2 = ibx; }
         else { ivn = ivz; ivt1 = ivx; ivt2 = ivy; ibn = ibz; ibt1 = ibx; ibt2 = iby; }
-        const double bx = A8(P, ibx, j, k, l), by = A8(P, iby, j, k, l), bz = A8(P, ibz, j, k, l);
-        const double vx = A8(P, ivx, j, k, l), vy = A8(P, ivy, j, k, l), vz = A8(P, ivz, j, k, l);
-        const double bsquare = (bx * bx + by * by) + bz * bz;
-        const double vdotb = (bx * vx + by * vy) + bz * vz;
-        const double vn = A8(P, ivn, j, k, l), p = A8(P, itau, j, k, l);
-        const double bn = A8(P, ibn, j, k, l);
+        const T bx = A8(P, ibx, j, k, l), by = A8(P, iby, j, k, l), bz = A8(P, ibz, j, k, l);
+        const T vx = A8(P, ivx, j, k, l), vy = A8(P, ivy, j, k, l), vz = A8(P, ivz, j, k, l);
+        const T bsquare = (bx * bx + by * by) + bz * bz;
+        const T vdotb = (bx * vx + by * vy) + bz * vz;
+        const T vn = A8(P, ivn, j, k, l), p = A8(P, itau, j, k, l);
+        const T bn = A8(P, ibn, j, k, l);
         for (int i = imin; i <= ibx - 1; ++i) A8(F, i, j, k, l) = A8(U, i, j, k, l) * vn;
         A8(F, ivn, j, k, l) = ((A8(F, ivn, j, k, l) + p) + 0.5 * bsquare) - bn * bn;
         A8(F, ivt1, j, k, l) = A8(F, ivt1, j, k, l) - bn * A8(P, ibt1, j, k, l);
@@ -374,22 +409,22 @@ struct Oracle {
     }
 
     // compute_signalspeed (solver/definition.f90:394-410)
-    static double signalspeed(double cs, double bn, double bt1, double bt2, double rho) {
-        const double a2 = cs * cs;
-        const double a4 = a2 * a2;
-        const double b2n = (bn * bn) / rho;
-        const double b2t1 = (bt1 * bt1) / rho;
-        const double b2t2 = (bt2 * bt2) / rho;
-        const double b2 = (b2n + b2t1) + b2t2;
-        const double b4 = b2 * b2;
-        return std::sqrt(0.5 * ((a2 + b2) + std::sqrt(MAX2(((a4 + b4) + (2.0 * b2) * a2) - (4.0 * a2) * b2n, 0.0))));
+    static T signalspeed(const T& cs, const T& bn, const T& bt1, const T& bt2, const T& rho) {
+        const T a2 = cs * cs;
+        const T a4 = a2 * a2;
+        const T b2n = (bn * bn) / rho;
+        const T b2t1 = (bt1 * bt1) / rho;
+        const T b2t2 = (bt2 * bt2) / rho;
+        const T b2 = (b2n + b2t1) + b2t2;
+        const T b4 = b2 * b2;
+        return sqrt_(0.5 * ((a2 + b2) + sqrt_(MAX2(((a4 + b4) + (2.0 * b2) * a2) - (4.0 * a2) * b2n, 0.0))));
     }
     // compute_roe (solver/definition.f90:387-392)
-    static double roe(double xl, double xr, double rl, double rr) {
-        return (std::sqrt(rl) * xl + std::sqrt(rr) * xr) / (std::sqrt(rl) + std::sqrt(rr));
+    static T roe(const T& xl, const T& xr, const T& rl, const T& rr) {
+        return (sqrt_(rl) * xl + sqrt_(rr) * xr) / (sqrt_(rl) + sqrt_(rr));
     }
     // compute_fluxhll (solver/definition.f90:380-385)
-    static double fluxhll(double yl, double yr, double xl, double xr, double sl, double sr) {
+    static T fluxhll(const T& yl, const T& yr, const T& xl, const T& xr, const T& sl, const T& sr) {
         return ((sr * yl - sl * yr) + (sl * sr) * (xr - xl)) / (sr - sl);
     }
 
@@ -399,23 +434,23 @@ struct Oracle {
         if (dir == x_dir) { ibn = ibx; ibt1 = iby; ibt2 = ibz; ivn = ivx; }
         else if (dir == y_dir) { ibn = iby; ibt1 = ibz; ibt2 = ibx; ivn = ivy; }
         else { ibn = ibz; ibt1 = ibx; ibt2 = iby; ivn = ivz; }
-        const double epsL = eos_epsilon(A8(primL, itau, j, k, l), A8(primL, irho, j, k, l));
-        const double epsR = eos_epsilon(A8(primR, itau, j, k, l), A8(primR, irho, j, k, l));
-        const double csL = eos_soundspeed(A8(primL, itau, j, k, l), A8(primL, irho, j, k, l));
-        const double csR = eos_soundspeed(A8(primR, itau, j, k, l), A8(primR, irho, j, k, l));
+        const T epsL = eos_epsilon(A8(primL, itau, j, k, l), A8(primL, irho, j, k, l));
+        const T epsR = eos_epsilon(A8(primR, itau, j, k, l), A8(primR, irho, j, k, l));
+        const T csL = eos_soundspeed(A8(primL, itau, j, k, l), A8(primL, irho, j, k, l));
+        const T csR = eos_soundspeed(A8(primR, itau, j, k, l), A8(primR, irho, j, k, l));
         ptou_face(primL, consL, j, k, l, epsL);
         ptou_face(primR, consR, j, k, l, epsR);
         ptof_side(primL, consL, fluxL, dir, j, k, l);
         ptof_side(primR, consR, fluxR, dir, j, k, l);
-        const double rhoL = A8(primL, irho, j, k, l), rhoR = A8(primR, irho, j, k, l);
-        const double cfsL = signalspeed(csL, A8(primL, ibn, j, k, l), A8(primL, ibt1, j, k, l),
+        const T rhoL = A8(primL, irho, j, k, l), rhoR = A8(primR, irho, j, k, l);
+        const T cfsL = signalspeed(csL, A8(primL, ibn, j, k, l), A8(primL, ibt1, j, k, l),
                                         A8(primL, ibt2, j, k, l), rhoL);
-        const double cfsR = signalspeed(csR, A8(primR, ibn, j, k, l), A8(primR, ibt1, j, k, l),
+        const T cfsR = signalspeed(csR, A8(primR, ibn, j, k, l), A8(primR, ibt1, j, k, l),
                                         A8(primR, ibt2, j, k, l), rhoR);
-        const double ubar = roe(A8(primL, ivn, j, k, l), A8(primR, ivn, j, k, l), rhoL, rhoR);
-        const double cbar = roe(cfsL, cfsR, rhoL, rhoR);
-        const double sL = MIN2(A8(primL, ivn, j, k, l) - cfsL, ubar - cbar);
-        const double sR = MAX2(A8(primR, ivn, j, k, l) + cfsR, ubar + cbar);
+        const T ubar = roe(A8(primL, ivn, j, k, l), A8(primR, ivn, j, k, l), rhoL, rhoR);
+        const T cbar = roe(cfsL, cfsR, rhoL, rhoR);
+        const T sL = MIN2(A8(primL, ivn, j, k, l) - cfsL, ubar - cbar);
+        const T sR = MAX2(A8(primR, ivn, j, k, l) + cfsR, ubar + cbar);
         if (sL >= 0.0) {
             for (int i = imin; i <= imax; ++i) A8(flux, i, j, k, l) = A8(fluxL, i, j, k, l);
         } else if (sL <= 0.0 && sR >= 0.0) {
@@ -452,8 +487,8 @@ struct Oracle {
                 for (int j = 1; j <= nx; ++j) {
                     double x, y, z;
                     get_coord(j, k, l, x, y, z);
-                    const double rho = A8(prim, irho, j, k, l);
-                    const double diff = rho - rho_floor;
+                    const T rho = A8(prim, irho, j, k, l);
+                    const T diff = rho - rho_floor;
                     const double factor = MAX2(SIGN1(diff), 0.0);
                     if (model == CUMC_MODEL_TORUS_SPH) {
                         const double dphidr = 1.0 / ((x - r_sh) * (x - r_sh));
@@ -613,8 +648,8 @@ struct Oracle {
         for (int l = 0; l <= nz + 1; ++l)
             for (int k = 0; k <= ny + 1; ++k)
                 for (int j = 0; j <= nx + 1; ++j) {
-                    const double vx = A8(prim, ivx, j, k, l), vy = A8(prim, ivy, j, k, l), vz = A8(prim, ivz, j, k, l);
-                    const double bx = B3(ibx, j, k, l), by = B3(iby, j, k, l), bz = B3(ibz, j, k, l);
+                    const T vx = A8(prim, ivx, j, k, l), vy = A8(prim, ivy, j, k, l), vz = A8(prim, ivz, j, k, l);
+                    const T bx = B3(ibx, j, k, l), by = B3(iby, j, k, l), bz = B3(ibz, j, k, l);
                     E3(ecell, iex, j, k, l) = vz * by - vy * bz;
                     E3(ecell, iey, j, k, l) = vx * bz - vz * bx;
                     E3(ecell, iez, j, k, l) = vy * bx - vx * by;
@@ -666,11 +701,11 @@ struct Oracle {
             for (int k = 0; k <= ny; ++k)
                 for (int j = 0; j <= nx; ++j) {
                     // PtoU_MHD (solver/ptou.f90:33-66)
-                    const double vx = A8(prim, ivx, j, k, l), vy = A8(prim, ivy, j, k, l), vz = A8(prim, ivz, j, k, l);
-                    const double bx = B3(ibx, j, k, l), by = B3(iby, j, k, l), bz = B3(ibz, j, k, l);
-                    const double rho = A8(prim, irho, j, k, l);
-                    const double vsquare = (vx * vx + vy * vy) + vz * vz;
-                    const double bsquare = (bx * bx + by * by) + bz * bz;
+                    const T vx = A8(prim, ivx, j, k, l), vy = A8(prim, ivy, j, k, l), vz = A8(prim, ivz, j, k, l);
+                    const T bx = B3(ibx, j, k, l), by = B3(iby, j, k, l), bz = B3(ibz, j, k, l);
+                    const T rho = A8(prim, irho, j, k, l);
+                    const T vsquare = (vx * vx + vy * vy) + vz * vz;
+                    const T bsquare = (bx * bx + by * by) + bz * bz;
                     A8(cons, irho, j, k, l) = rho;
                     A8(cons, ivx, j, k, l) = vx * rho;
                     A8(cons, ivy, j, k, l) = vy * rho;
@@ -694,16 +729,16 @@ struct Oracle {
             for (int k = 0; k <= ny; ++k)
                 for (int j = 0; j <= nx; ++j) {
                     // UtoP_MHD (solver/utop.f90:33-68)
-                    const double rho = A8(cons, irho, j, k, l);
+                    const T rho = A8(cons, irho, j, k, l);
                     A8(prim, irho, j, k, l) = rho;
                     A8(prim, ivx, j, k, l) = A8(cons, ivx, j, k, l) / rho;
                     A8(prim, ivy, j, k, l) = A8(cons, ivy, j, k, l) / rho;
                     A8(prim, ivz, j, k, l) = A8(cons, ivz, j, k, l) / rho;
                     for (int i = ibx; i <= ibz; ++i) A8(prim, i, j, k, l) = A8(cons, i, j, k, l);
-                    const double bx = B3(ibx, j, k, l), by = B3(iby, j, k, l), bz = B3(ibz, j, k, l);
-                    const double vx = A8(prim, ivx, j, k, l), vy = A8(prim, ivy, j, k, l), vz = A8(prim, ivz, j, k, l);
-                    const double bsquare = (bx * bx + by * by) + bz * bz;
-                    const double vsquare = (vx * vx + vy * vy) + vz * vz;
+                    const T bx = B3(ibx, j, k, l), by = B3(iby, j, k, l), bz = B3(ibz, j, k, l);
+                    const T vx = A8(prim, ivx, j, k, l), vy = A8(prim, ivy, j, k, l), vz = A8(prim, ivz, j, k, l);
+                    const T bsquare = (bx * bx + by * by) + bz * bz;
+                    const T vsquare = (vx * vx + vy * vy) + vz * vz;
                     EPS(j, k, l) = (A8(cons, itau, j, k, l) - 0.5 * bsquare) / rho - 0.5 * vsquare;
                 }
     }
@@ -865,8 +900,8 @@ struct Oracle {
             for (int k = 0; k <= ny; ++k)
                 for (int j = 0; j <= nx; ++j)
                     for (int i = imin; i <= imax; ++i) {
-                        double& c = A8(cons, i, j, k, l);
-                        const double u0 = A8(u_old, i, j, k, l), L = A8(l_rk, i, j, k, l);
+                        T& c = A8(cons, i, j, k, l);
+                        const T u0 = A8(u_old, i, j, k, l), L = A8(l_rk, i, j, k, l);
                         if (stage == 1) c = u0 + dt * L;
                         else if (stage == 2) c = (rk20 * u0 + rk21 * c) + (rk22 * dt) * L;
                         else c = (rk30 * u0 + rk31 * c) + (rk32 * dt) * L;
@@ -900,22 +935,22 @@ struct Oracle {
         for (int l = 1; l <= nz; ++l)
             for (int k = 1; k <= ny; ++k)
                 for (int j = 1; j <= nx; ++j) {
-                    const double rho = A8(prim, irho, j, k, l);
-                    const double cs = eos_soundspeed(A8(prim, itau, j, k, l), rho);
+                    const double rho = val(A8(prim, irho, j, k, l));
+                    const double cs = std::sqrt((ggas * val(A8(prim, itau, j, k, l))) / rho);
                     const double a2 = cs * cs;
                     const double a4 = a2 * a2;
-                    const double b2x = (B3(ibx, j, k, l) * B3(ibx, j, k, l)) / rho;
-                    const double b2y = (B3(iby, j, k, l) * B3(iby, j, k, l)) / rho;
-                    const double b2z = (B3(ibz, j, k, l) * B3(ibz, j, k, l)) / rho;
+                    const double b2x = (val(B3(ibx, j, k, l)) * val(B3(ibx, j, k, l))) / rho;
+                    const double b2y = (val(B3(iby, j, k, l)) * val(B3(iby, j, k, l))) / rho;
+                    const double b2z = (val(B3(ibz, j, k, l)) * val(B3(ibz, j, k, l))) / rho;
                     const double b2 = (b2x + b2y) + b2z;
                     const double b4 = b2 * b2;
                     const double base = (a4 + (2.0 * a2) * b2) + b4;
                     const double cfx = std::sqrt(0.5 * ((a2 + b2) + std::sqrt(base - (4.0 * a2) * b2x)));
                     const double cfy = std::sqrt(0.5 * ((a2 + b2) + std::sqrt(base - (4.0 * a2) * b2y)));
                     const double cfz = std::sqrt(0.5 * ((a2 + b2) + std::sqrt(base - (4.0 * a2) * b2z)));
-                    const double lambda = MAX3(std::fabs(A8(prim, ivx, j, k, l)) + cfx,
-                                               std::fabs(A8(prim, ivy, j, k, l)) + cfy,
-                                               std::fabs(A8(prim, ivz, j, k, l)) + cfz);
+                    const double lambda = MAX3(std::fabs(val(A8(prim, ivx, j, k, l))) + cfx,
+                                               std::fabs(val(A8(prim, ivy, j, k, l))) + cfy,
+                                               std::fabs(val(A8(prim, ivz, j, k, l))) + cfz);
                     double dxl, dyl, dzl, x, y, z;
                     coord_dx(j, k, l, dxl, dyl, dzl);
                     get_coord(j, k, l, x, y, z);
@@ -940,9 +975,9 @@ struct Oracle {
                 for (int j = 1; j <= nx; ++j) {
                     double axp, axm, ayp, aym, azp, azm;
                     geom_area(j, k, l, axp, axm, ayp, aym, azp, azm);
-                    const double div_b = ((axp * A8(prim, ibx, j, k, l) - axm * A8(prim, ibx, j - 1, k, l)) +
-                                          (ayp * A8(prim, iby, j, k, l) - aym * A8(prim, iby, j, k - 1, l))) +
-                                         (azp * A8(prim, ibz, j, k, l) - azm * A8(prim, ibz, j, k, l - 1));
+                    const double div_b = ((axp * val(A8(prim, ibx, j, k, l)) - axm * val(A8(prim, ibx, j - 1, k, l))) +
+                                          (ayp * val(A8(prim, iby, j, k, l)) - aym * val(A8(prim, iby, j, k - 1, l)))) +
+                                         (azp * val(A8(prim, ibz, j, k, l)) - azm * val(A8(prim, ibz, j, k, l - 1)));
                     maxdb = MAX2(maxdb, div_b);
                 }
         return maxdb;
@@ -988,14 +1023,16 @@ struct Oracle {
         yF.assign(c->yf, c->yf + ny + 7);
         zF.assign(c->zf, c->zf + nz + 7);
         for (auto* v : {&prim, &cons, &primL, &primR, &consL, &consR, &fluxL, &fluxR, &flux, &l_rk, &u_old, &sc})
-            v->assign(8 * NT, 0.0);
-        bcell.assign(3 * NT, 0.0);
-        ecell.assign(3 * NT, 0.0);
-        ecorn.assign(3 * NT, 0.0);
-        eps.assign(NT, 0.0);
+            v->assign(8 * NT, T(0.0));
+        bcell.assign(3 * NT, T(0.0));
+        ecell.assign(3 * NT, T(0.0));
+        ecorn.assign(3 * NT, T(0.0));
+        eps.assign(NT, T(0.0));
         return true;
     }
 };
+using Oracle = OracleT<double>;
+using OracleTL = OracleT<Dual>;
 
 }  // namespace
 
@@ -1039,6 +1076,38 @@ int orc_download(void* h, double* prim, double* cons, double* eps, double* bcell
     if (eps) std::memcpy(eps, o->eps.data(), sizeof(double) * o->NT);
     if (bcell) std::memcpy(bcell, o->bcell.data(), sizeof(double) * 3 * o->NT);
     if (lrk) std::memcpy(lrk, o->l_rk.data(), sizeof(double) * 8 * o->NT);
+    return 0;
+}
+
+// tangent-linear oracle: the same map on (value, direction) pairs
+void* orc_tl_create(const cumc_config* cfg, char* err, int errlen) {
+    auto* o = new OracleTL();
+    if (!o->setup(cfg, err, errlen)) { delete o; return nullptr; }
+    return o;
+}
+void orc_tl_free(void* h) { delete static_cast<OracleTL*>(h); }
+int orc_tl_upload(void* h, const double* prim, const double* eps, const double* dprim, const double* deps) {
+    auto* o = static_cast<OracleTL*>(h);
+    for (size_t i = 0; i < 8 * o->NT; ++i) o->prim[i] = Dual(prim[i], dprim[i]);
+    for (size_t i = 0; i < o->NT; ++i) o->eps[i] = Dual(eps[i], deps[i]);
+    return 0;
+}
+int orc_tl_initial_update(void* h) { static_cast<OracleTL*>(h)->initial_update(); return 0; }
+int orc_tl_rungekutta(void* h, double dt) { static_cast<OracleTL*>(h)->rungekutta(dt); return 0; }
+// values and derivatives of prim, cons, eps, bcell; any pointer may be NULL
+int orc_tl_download(void* h, double* prim, double* cons, double* eps, double* bcell, double* dprim, double* dcons,
+                    double* deps, double* dbcell) {
+    auto* o = static_cast<OracleTL*>(h);
+    auto put = [](const std::vector<Dual>& a, double* v, double* d) {
+        for (size_t i = 0; i < a.size(); ++i) {
+            if (v) v[i] = a[i].v;
+            if (d) d[i] = a[i].d;
+        }
+    };
+    put(o->prim, prim, dprim);
+    put(o->cons, cons, dcons);
+    put(o->eps, eps, deps);
+    put(o->bcell, bcell, dbcell);
     return 0;
 }
 

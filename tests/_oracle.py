@@ -135,3 +135,65 @@ class Oracle:
             self.step(total_time)
             n += 1
         return n
+
+
+class TangentOracle:
+    """Tangent-linear run of the oracle: the same discrete map on
+    (value, direction) pairs with every branch frozen at the base point, so
+    the derivative parts are the exact directional derivative of the map
+    upload -> initial_update -> RK3 steps (the FP64 reference gradient the
+    adjoint is checked against)."""
+
+    def __init__(self, problem: Problem, threads: int | None = None):
+        self.problem = problem
+        L = self._L = lib(ORACLE_LIB)
+        if not hasattr(L.orc_tl_create, "_typed"):
+            dp = POINTER(c_double)
+            L.orc_tl_create.restype = c_void_p
+            L.orc_tl_create.argtypes = [POINTER(N.CumcConfig), c_char_p, c_int]
+            L.orc_tl_free.argtypes = [c_void_p]
+            L.orc_tl_upload.argtypes = [c_void_p, dp, dp, dp, dp]
+            L.orc_tl_initial_update.argtypes = [c_void_p]
+            L.orc_tl_rungekutta.argtypes = [c_void_p, c_double]
+            L.orc_tl_download.argtypes = [c_void_p] + [dp] * 8
+            L.orc_tl_create._typed = True
+        if threads:
+            L.orc_set_threads(int(threads))
+        self._cfg = problem.config()
+        err = ctypes.create_string_buffer(512)
+        h = L.orc_tl_create(ctypes.byref(self._cfg), err, 512)
+        if not h:
+            raise ValueError(err.value.decode())
+        self._h = h
+
+    def close(self):
+        if self._h:
+            self._L.orc_tl_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        p = self.problem
+        return (p.nz + 6, p.ny + 6, p.nx + 6)
+
+    def run(self, dprim: np.ndarray, deps: np.ndarray, dts) -> tuple[dict, dict]:
+        """initial_update and one rungekutta per dt from the problem's state
+        perturbed along (dprim, deps); returns (values, derivatives)."""
+        p = self.problem
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (p.prim, p.eps, dprim, deps)]
+        self._L.orc_tl_upload(self._h, *[_dp(a) for a in arrs])
+        self._L.orc_tl_initial_update(self._h)
+        for dt in dts:
+            self._L.orc_tl_rungekutta(self._h, float(dt))
+        v = {"prim": np.zeros(self.shape + (8,)), "cons": np.zeros(self.shape + (8,)), "eps": np.zeros(self.shape),
+             "bcell": np.zeros(self.shape + (3,))}
+        d = {k: np.zeros_like(a) for k, a in v.items()}
+        self._L.orc_tl_download(self._h, _dp(v["prim"]), _dp(v["cons"]), _dp(v["eps"]), _dp(v["bcell"]),
+                                _dp(d["prim"]), _dp(d["cons"]), _dp(d["eps"]), _dp(d["bcell"]))
+        return v, d
