@@ -23,6 +23,7 @@
 // their sources and then zero.
 #pragma once
 #include "cumc_kernels.cuh"
+#include "cumc_walk.cuh"
 
 namespace cumc {
 
@@ -147,20 +148,24 @@ __device__ __forceinline__ void recon_adj(const AxisTabs& A, int c, const double
 // ---------------------------------------------------------------------------
 template <int DIR>
 struct SideAdj {
-    double rho, v[3], p, b[3], e, vsq, bsq, E, hb2, vdotb;
+    // forward values here only weight derivatives, so reciprocals replace
+    // the forward's divisions (no branch depends on them)
+    double rho, irho, v[3], p, b[3], e, vsq, bsq, E, hb2, vdotb;
     double Lrho, Lv[3], Lp, Lb[3], LE, Lhb2, Lvdotb;
-    __device__ __forceinline__ void init(const double w[8], double g) {
+    __device__ __forceinline__ void init(const double w[8], double ig1) {
         rho = w[IRHO];
+        irho = 1.0 / rho;
         v[0] = w[IVX]; v[1] = w[IVY]; v[2] = w[IVZ];
         p = w[ITAU];
         b[0] = w[IBX]; b[1] = w[IBY]; b[2] = w[IBZ];
-        e = (p / rho) / (g - 1.0);
+        e = (p * irho) * ig1;
         vsq = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
         bsq = (b[0] * b[0] + b[1] * b[1]) + b[2] * b[2];
         E = rho * (e + 0.5 * vsq) + 0.5 * bsq;
         hb2 = 0.5 * bsq;
         vdotb = (b[0] * v[0] + b[1] * v[1]) + b[2] * v[2];
         Lrho = Lp = LE = Lhb2 = Lvdotb = 0.0;
+#pragma unroll
         for (int i = 0; i < 3; ++i) Lv[i] = Lb[i] = 0.0;
     }
     __device__ __forceinline__ double u(int q) const {
@@ -217,17 +222,18 @@ struct SideAdj {
         }
     }
     // fold E, hb2, vdotb, e into the primitive adjoints; out[8] in natural order
-    __device__ __forceinline__ void finish(double g, double out[8]) {
+    __device__ __forceinline__ void finish(double ig1, double out[8]) {
         const double Le = LE * rho;
         const double Lvsq = LE * 0.5 * rho;
         const double Lbsq = LE * 0.5 + 0.5 * Lhb2;
         Lrho += LE * (e + 0.5 * vsq);
+#pragma unroll
         for (int i = 0; i < 3; ++i) {
             Lb[i] += Lvdotb * v[i] + 2.0 * b[i] * Lbsq;
             Lv[i] += Lvdotb * b[i] + 2.0 * v[i] * Lvsq;
         }
-        Lp += Le / (rho * (g - 1.0));
-        Lrho -= Le * e / rho;
+        Lp += Le * irho * ig1;
+        Lrho -= Le * e * irho;
         out[IRHO] += Lrho;
         out[IVX] += Lv[0]; out[IVY] += Lv[1]; out[IVZ] += Lv[2];
         out[ITAU] += Lp;
@@ -236,30 +242,29 @@ struct SideAdj {
 };
 
 // adjoint of cf = signalspeed(cs, bn, bt1, bt2, rho): adds to the arguments' adjoints
-__device__ __forceinline__ void signalspeed_adj(double cs, double bn, double bt1, double bt2, double rho, double lcf,
-                                                double& lcs, double& lbn, double& lbt1, double& lbt2, double& lrho) {
-    if (lcf == 0.0) return;
+__device__ __forceinline__ void signalspeed_adj(double cs, double bn, double bt1, double bt2, double rho, double cf,
+                                                double lcf, double& lcs, double& lbn, double& lbt1, double& lbt2,
+                                                double& lrho) {
+    if (lcf == 0.0 || !(cf > 0.0)) return;
+    const double irho = 1.0 / rho;
     const double a2 = cs * cs;
-    const double b2n = (bn * bn) / rho, b2t1 = (bt1 * bt1) / rho, b2t2 = (bt2 * bt2) / rho;
+    const double b2n = (bn * bn) * irho, b2t1 = (bt1 * bt1) * irho, b2t2 = (bt2 * bt2) * irho;
     const double b2 = (b2n + b2t1) + b2t2;
     const double inner = ((a2 * a2 + b2 * b2) + (2.0 * b2) * a2) - (4.0 * a2) * b2n;
-    const double s = sqrt(fmax(inner, 0.0));
-    const double cf = sqrt(0.5 * ((a2 + b2) + s));
-    if (!(cf > 0.0)) return;
     const double lsum = lcf * 0.25 / cf;  // d cf / d (a2 + b2 + s)
     double la2 = lsum, lb2 = lsum, lb2n = 0.0;
     if (inner > 0.0) {
-        const double ls = lsum / (2.0 * s);  // d s / d inner
+        const double ls = lsum * 0.5 / sqrt(inner);  // d sqrt(inner) / d inner
         la2 += ls * (2.0 * (a2 + b2) - 4.0 * b2n);
         lb2 += ls * 2.0 * (a2 + b2);
         lb2n += ls * (-4.0 * a2);
     }
     lb2n += lb2;
     lcs += 2.0 * cs * la2;
-    lbn += 2.0 * bn / rho * lb2n;
-    lbt1 += 2.0 * bt1 / rho * lb2;
-    lbt2 += 2.0 * bt2 / rho * lb2;
-    lrho -= (b2n * lb2n + (b2t1 + b2t2) * lb2) / rho;
+    lbn += 2.0 * bn * irho * lb2n;
+    lbt1 += 2.0 * bt1 * irho * lb2;
+    lbt2 += 2.0 * bt2 * irho * lb2;
+    lrho -= (b2n * lb2n + (b2t1 + b2t2) * lb2) * irho;
 }
 
 // adjoint of out[7] = hll_flux7<DIR>(wl, wr): lout[7] -> lwl[8], lwr[8] (added)
@@ -271,9 +276,10 @@ __device__ __forceinline__ void hll_adj(const double wl[8], const double wr[8], 
     constexpr int bt_a = DIR == 0 ? IBY : IBX;
     constexpr int bt_b = DIR == 2 ? IBY : IBZ;
     const int comp[7] = {IRHO, IVX, IVY, IVZ, ITAU, bt_a, bt_b};
+    const double ig1 = 1.0 / (g - 1.0);
     SideAdj<DIR> L, R;
-    L.init(wl, g);
-    R.init(wr, g);
+    L.init(wl, ig1);
+    R.init(wr, ig1);
     const double csL = sqrt((g * wl[ITAU]) / wl[IRHO]);
     const double csR = sqrt((g * wr[ITAU]) / wr[IRHO]);
     const double cfL = signalspeed(csL, wl[ibn], wl[ibt1], wl[ibt2], wl[IRHO]);
@@ -286,16 +292,18 @@ __device__ __forceinline__ void hll_adj(const double wl[8], const double wr[8], 
     const double sL = fmin(aL, bL), sR = fmax(aR, bR);
     double lsL = 0.0, lsR = 0.0;
     if (sL >= 0.0) {
+#pragma unroll
         for (int c = 0; c < 7; ++c) L.f_adj(comp[c], lout[c]);
     } else if (sL <= 0.0 && sR >= 0.0) {
-        const double d = sR - sL;
+        const double id = 1.0 / (sR - sL);
         double ld = 0.0;
+#pragma unroll
         for (int c = 0; c < 7; ++c) {
             const int q = comp[c];
             const double fl = L.f(q), fr = R.f(q), ul = L.u(q), ur = R.u(q);
-            const double out = ((sR * fl - sL * fr) + (sL * sR) * (ur - ul)) / d;
-            const double ln = lout[c] / d;
-            ld -= lout[c] * out / d;
+            const double out = ((sR * fl - sL * fr) + (sL * sR) * (ur - ul)) * id;
+            const double ln = lout[c] * id;
+            ld -= ln * out;
             L.f_adj(q, sR * ln);
             R.f_adj(q, -sL * ln);
             R.u_adj(q, sL * sR * ln);
@@ -306,6 +314,7 @@ __device__ __forceinline__ void hll_adj(const double wl[8], const double wr[8], 
         lsR += ld;
         lsL -= ld;
     } else {
+#pragma unroll
         for (int c = 0; c < 7; ++c) R.f_adj(comp[c], lout[c]);
     }
     // sL = min(aL, bL), sR = max(aR, bR)
@@ -313,34 +322,36 @@ __device__ __forceinline__ void hll_adj(const double wl[8], const double wr[8], 
     if (aL <= bL) { lvnL += lsL; lcfL -= lsL; } else { lubar += lsL; lcbar -= lsL; }
     if (aR >= bR) { lvnR += lsR; lcfR += lsR; } else { lubar += lsR; lcbar += lsR; }
     // Roe averages
-    const double ssum = sqL + sqR;
-    double lsqL = (lubar * (wl[ivn] - ubar) + lcbar * (cfL - cbar)) / ssum;
-    double lsqR = (lubar * (wr[ivn] - ubar) + lcbar * (cfR - cbar)) / ssum;
-    lvnL += lubar * sqL / ssum;
-    lvnR += lubar * sqR / ssum;
-    lcfL += lcbar * sqL / ssum;
-    lcfR += lcbar * sqR / ssum;
+    const double iss = 1.0 / (sqL + sqR);
+    double lsqL = (lubar * (wl[ivn] - ubar) + lcbar * (cfL - cbar)) * iss;
+    double lsqR = (lubar * (wr[ivn] - ubar) + lcbar * (cfR - cbar)) * iss;
+    lvnL += lubar * sqL * iss;
+    lvnR += lubar * sqR * iss;
+    lcfL += lcbar * sqL * iss;
+    lcfR += lcbar * sqR * iss;
     // fast speeds
     double lcsL = 0.0, lcsR = 0.0;
-    signalspeed_adj(csL, wl[ibn], wl[ibt1], wl[ibt2], wl[IRHO], lcfL, lcsL, L.Lb[DIR], L.Lb[(DIR + 1) % 3],
+    signalspeed_adj(csL, wl[ibn], wl[ibt1], wl[ibt2], wl[IRHO], cfL, lcfL, lcsL, L.Lb[DIR], L.Lb[(DIR + 1) % 3],
                     L.Lb[(DIR + 2) % 3], L.Lrho);
-    signalspeed_adj(csR, wr[ibn], wr[ibt1], wr[ibt2], wr[IRHO], lcfR, lcsR, R.Lb[DIR], R.Lb[(DIR + 1) % 3],
+    signalspeed_adj(csR, wr[ibn], wr[ibt1], wr[ibt2], wr[IRHO], cfR, lcfR, lcsR, R.Lb[DIR], R.Lb[(DIR + 1) % 3],
                     R.Lb[(DIR + 2) % 3], R.Lrho);
-    // cs = sqrt(g p / rho), sq = sqrt(rho)
+    // cs = sqrt(g p / rho): d cs = cs/2 (dp/p - drho/rho); sq = sqrt(rho): d sq = drho / (2 sq)
     if (csL > 0.0) {
-        L.Lp += lcsL * g / (2.0 * csL * wl[IRHO]);
-        L.Lrho -= lcsL * csL / (2.0 * wl[IRHO]);
+        const double h = 0.5 * lcsL * csL;
+        L.Lp += h / wl[ITAU];
+        L.Lrho -= h * L.irho;
     }
     if (csR > 0.0) {
-        R.Lp += lcsR * g / (2.0 * csR * wr[IRHO]);
-        R.Lrho -= lcsR * csR / (2.0 * wr[IRHO]);
+        const double h = 0.5 * lcsR * csR;
+        R.Lp += h / wr[ITAU];
+        R.Lrho -= h * R.irho;
     }
-    L.Lrho += lsqL / (2.0 * sqL);
-    R.Lrho += lsqR / (2.0 * sqR);
+    L.Lrho += 0.5 * lsqL / sqL;
+    R.Lrho += 0.5 * lsqR / sqR;
     L.Lv[DIR] += lvnL;
     R.Lv[DIR] += lvnR;
-    L.finish(g, lwl);
-    R.finish(g, lwr);
+    L.finish(ig1, lwl);
+    R.finish(ig1, lwr);
 }
 
 // ---------------------------------------------------------------------------
@@ -420,14 +431,20 @@ __global__ void __launch_bounds__(256) k_adj_ecell(Box b, Prim pr, const double*
     o.bc[2][i] += ly * vx - lx * vy;
 }
 
-// sweep^T: per face (normal 0:n_d, transverse 0:n+1), the flux adjoints from
-// mu (flux difference) and the edge adjoints (emf), then HLL^T and the
-// reconstruction transposes of the two adjacent cells, accumulated into the
-// primitive adjoints of cells c-2..c+3 (atomically: neighbouring faces share
-// cells) and into the normal-field adjoint of the face (lambf).
+// adjoints of the reconstructed left and right states of each face (the 7
+// reconstructed fields in sweep order), stored at the face's left cell
+struct FaceAdj {
+    double* l[7];
+    double* r[7];
+};
+
+// sweep^T, pass A: per face (normal 0:n_d, transverse 0:n+1), the flux
+// adjoints from mu (flux difference) and the edge adjoints (emf), the forward
+// left/right states, and HLL^T. Writes the state adjoints to fa and adds the
+// normal-field adjoint of the face to lambf.
 template <int DIR, int RECON>
-__global__ void __launch_bounds__(128) k_adj_sweep(Box b, Tabs T, Prim pr, double ggas, AdjStage a, AdjPrim o,
-                                                  double* lambf) {
+__global__ void __launch_bounds__(128) k_adj_hll(Box b, Tabs T, Prim pr, double ggas, AdjStage a, FaceAdj fa,
+                                                double* lambf) {
     const int n0 = (DIR == 0 ? b.nx : b.nx + 1) + 1;
     const int n1 = (DIR == 1 ? b.ny : b.ny + 1) + 1;
     const int n2 = (DIR == 2 ? b.nz : b.nz + 1) + 1;
@@ -473,36 +490,40 @@ __global__ void __launch_bounds__(128) k_adj_sweep(Box b, Tabs T, Prim pr, doubl
     bool any = false;
 #pragma unroll
     for (int q = 0; q < 7; ++q) any |= lf[q] != 0.0;
-    if (!any) return;
+    if (!any) {
+#pragma unroll
+        for (int v = 0; v < 7; ++v) fa.l[v][base] = fa.r[v][base] = 0.0;
+        return;
+    }
 
     constexpr int bt_a = DIR == 0 ? 1 : 0;
     constexpr int bt_b = DIR == 2 ? 1 : 2;
     const double* src[7] = {pr.w[0], pr.w[1], pr.w[2], pr.w[3], pr.w[4], pr.bc[bt_a], pr.bc[bt_b]};
-    double* dst[7] = {o.w[0], o.w[1], o.w[2], o.w[3], o.w[4], o.bc[bt_a], o.bc[bt_b]};
     const int slot[7] = {IRHO, IVX, IVY, IVZ, ITAU, IBX + bt_a, IBX + bt_b};
 
-    // forward states
-    double wl[8], wr[8], cv[7][6];
+    // forward states (the forward sweep's values: vp_out of cell c, vm_out of cell c+1)
+    double wl[8], wr[8];
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
         const double* q = src[v] + base;
+        double cv[6];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) cv[v][m] = q[(m - 2) * s];  // cells c-2..c+3
+        for (int m = 0; m < 6; ++m) cv[m] = q[(m - 2) * s];  // cells c-2..c+3
         double vm, vp;
         if (RECON == 4) {
-            const double dmm = ppm_slope(cv[v][0], cv[v][1], cv[v][2], A.s0[c - 1], A.s1[c - 1]);
-            const double dmc = ppm_slope(cv[v][1], cv[v][2], cv[v][3], A.s0[c], A.s1[c]);
-            const double dmp = ppm_slope(cv[v][2], cv[v][3], cv[v][4], A.s0[c + 1], A.s1[c + 1]);
-            const double dmq = ppm_slope(cv[v][3], cv[v][4], cv[v][5], A.s0[c + 2], A.s1[c + 2]);
-            const double V0 = ppm_face(cv[v][1], cv[v][2], dmm, dmc, A.a0[c - 1], A.a1[c - 1], A.a2[c - 1], A.a3[c - 1]);
-            const double V1 = ppm_face(cv[v][2], cv[v][3], dmc, dmp, A.a0[c], A.a1[c], A.a2[c], A.a3[c]);
-            const double V2 = ppm_face(cv[v][3], cv[v][4], dmp, dmq, A.a0[c + 1], A.a1[c + 1], A.a2[c + 1], A.a3[c + 1]);
+            const double dmm = ppm_slope(cv[0], cv[1], cv[2], A.s0[c - 1], A.s1[c - 1]);
+            const double dmc = ppm_slope(cv[1], cv[2], cv[3], A.s0[c], A.s1[c]);
+            const double dmp = ppm_slope(cv[2], cv[3], cv[4], A.s0[c + 1], A.s1[c + 1]);
+            const double dmq = ppm_slope(cv[3], cv[4], cv[5], A.s0[c + 2], A.s1[c + 2]);
+            const double V0 = ppm_face(cv[1], cv[2], dmm, dmc, A.a0[c - 1], A.a1[c - 1], A.a2[c - 1], A.a3[c - 1]);
+            const double V1 = ppm_face(cv[2], cv[3], dmc, dmp, A.a0[c], A.a1[c], A.a2[c], A.a3[c]);
+            const double V2 = ppm_face(cv[3], cv[4], dmp, dmq, A.a0[c + 1], A.a1[c + 1], A.a2[c + 1], A.a3[c + 1]);
             double vm0, vp1;
-            ppm_fix(cv[v][2], V0, V1, vm0, vp);
-            ppm_fix(cv[v][3], V1, V2, vm, vp1);
+            ppm_fix(cv[2], V0, V1, vm0, vp);
+            ppm_fix(cv[3], V1, V2, vm, vp1);
         } else {
-            vp = cv[v][2] + 0.5 * tvd_slope(cv[v][1], cv[v][2], cv[v][3], A.tcf[c], A.tcb[c]);
-            vm = cv[v][3] - 0.5 * tvd_slope(cv[v][2], cv[v][3], cv[v][4], A.tcf[c + 1], A.tcb[c + 1]);
+            vp = cv[2] + 0.5 * tvd_slope(cv[1], cv[2], cv[3], A.tcf[c], A.tcb[c]);
+            vm = cv[3] - 0.5 * tvd_slope(cv[2], cv[3], cv[4], A.tcf[c + 1], A.tcb[c + 1]);
         }
         wl[slot[v]] = vp;
         wr[slot[v]] = vm;
@@ -514,16 +535,119 @@ __global__ void __launch_bounds__(128) k_adj_sweep(Box b, Tabs T, Prim pr, doubl
     double lwl[8] = {0, 0, 0, 0, 0, 0, 0, 0}, lwr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     hll_adj<DIR>(wl, wr, ggas, lf, lwl, lwr);
     lambf[base] += lwl[IBX + DIR] + lwr[IBX + DIR];
-
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
-        double lv[6] = {0, 0, 0, 0, 0, 0};
-        recon_adj<RECON>(A, c, &cv[v][0], 0.0, lwl[slot[v]], &lv[0]);      // vp_out of cell c
-        recon_adj<RECON>(A, c + 1, &cv[v][1], lwr[slot[v]], 0.0, &lv[1]);  // vm_out of cell c+1
-#pragma unroll
-        for (int m = 0; m < 6; ++m)
-            if (lv[m] != 0.0) atomicAdd(dst[v] + base + (m - 2) * s, lv[m]);
+        fa.l[v][base] = lwl[slot[v]];
+        fa.r[v][base] = lwr[slot[v]];
     }
+}
+
+// field v (0..6) of a sweep along DIR: source and adjoint arrays
+template <int DIR>
+__device__ __forceinline__ void sweep_field(const Prim& pr, const AdjPrim& o, int v, const double*& src, double*& dst) {
+    constexpr int bt_a = DIR == 0 ? 1 : 0;
+    constexpr int bt_b = DIR == 2 ? 1 : 2;
+    if (v < 5) {
+        src = pr.w[v];
+        dst = o.w[v];
+    } else {
+        src = pr.bc[v == 5 ? bt_a : bt_b];
+        dst = o.bc[v == 5 ? bt_a : bt_b];
+    }
+}
+
+// sweep^T, pass B along y or z: the reconstruction transpose. One thread
+// per (column, field, segment of RC_SEG cells) walks its segment: cell c's
+// reconstruction (vm_out, vp_out) took its seeds from faces c-1 and c; its
+// transpose adds to cells c-2..c+2, kept in a five-cell ring, and a cell is
+// complete once the walk has passed it by two. The four cells next to each
+// end of a segment also receive from the neighbouring segment and are added
+// atomically; the rest with a plain add (no other thread writes them in this
+// launch). The next cell and face seeds are loaded one cell ahead.
+constexpr int RC_SEG = 32;
+
+template <int DIR, int RECON>
+__global__ void __launch_bounds__(128) k_adj_recon_col(Box b, Tabs T, Prim pr, FaceAdj fa, AdjPrim o) {
+    using G = WalkGeom<DIR>;
+    const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= G::ncols(b)) return;
+    const int v = blockIdx.y;
+    const int nd = G::nd(b);
+    const int c0 = blockIdx.z * RC_SEG;
+    if (c0 > nd + 1) return;
+    const int c1 = min(c0 + RC_SEG, nd + 2);  // reconstructed cells 0..nd+1
+    const int a = (int)(col % G::wa(b)), cc = (int)(col / G::wa(b));
+    const int s = G::stride(b);
+    const int base = G::idx(b, a, cc, 0);
+    const AxisTabs A = T.ax[DIR];
+    const double* src;
+    double* dst;
+    sweep_field<DIR>(pr, o, v, src, dst);
+    src += base;
+    dst += base;
+    const double* fl = fa.l[v] + base;
+    const double* fr = fa.r[v] + base;
+    auto emit = [&](int q, double val, bool shared) {
+        if (val == 0.0) return;
+        if (shared) atomicAdd(dst + q * s, val);
+        else dst[q * s] += val;
+    };
+    double x[5] = {src[(c0 - 2) * s], src[(c0 - 1) * s], src[c0 * s], src[(c0 + 1) * s], src[(c0 + 2) * s]};
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // cells c-2..c+2
+    double lvm = c0 >= 1 ? fr[(c0 - 1) * s] : 0.0;
+    double lvp = c0 <= nd ? fl[c0 * s] : 0.0;
+    for (int c = c0; c < c1; ++c) {
+        const double xn = c + 3 <= nd + 3 ? src[(c + 3) * s] : 0.0;
+        const double lvm_n = fr[c * s];  // face c seeds vm_out of cell c+1
+        const double lvp_n = c + 1 <= nd ? fl[(c + 1) * s] : 0.0;
+        recon_adj<RECON>(A, c, x, lvm, lvp, acc);
+        emit(c - 2, acc[0], c - 2 <= c0 + 1);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            acc[m] = acc[m + 1];
+            x[m] = x[m + 1];
+        }
+        acc[4] = 0.0;
+        x[4] = xn;
+        lvm = lvm_n;
+        lvp = lvp_n;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) emit(c1 - 2 + m, acc[m], true);
+}
+
+// sweep^T, pass B along x: the reconstruction transpose with one lane per
+// cell. A warp covers cells 28w-4 .. 28w+27 of a row and owns the middle 28
+// (lanes 2..29): each lane transposes its own cell's reconstruction, and the
+// five contributions to each owned cell are summed through warp shuffles.
+template <int RECON>
+__global__ void __launch_bounds__(128) k_adj_recon_x(Box b, Tabs T, Prim pr, FaceAdj fa, AdjPrim o) {
+    const int nw = (b.nx + 6 + 27) / 28;  // warps per row
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long rows = (long long)(b.ny + 2) * (b.nz + 2);
+    if (warp >= rows * nw) return;  // whole warp
+    const int v = blockIdx.y;
+    const int w = (int)(warp % nw);
+    const long long row = warp / nw;
+    const int k = (int)(row % (b.ny + 2)), l = (int)(row / (b.ny + 2));
+    const int c = 28 * w + lane - 4;
+    const AxisTabs A = T.ax[0];
+    const double* src;
+    double* dst;
+    sweep_field<0>(pr, o, v, src, dst);
+    const int base = b.idx(0, k, l);
+    double lv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (c >= 0 && c <= b.nx + 1) {
+        const double* q = src + base + c;
+        const double x[5] = {q[-2], q[-1], q[0], q[1], q[2]};
+        const double lvm = c >= 1 ? fa.r[v][base + c - 1] : 0.0;
+        const double lvp = c <= b.nx ? fa.l[v][base + c] : 0.0;
+        recon_adj<RECON>(A, c, x, lvm, lvp, lv);
+    }
+    const double tot = lv[2] + __shfl_down_sync(0xffffffffu, lv[0], 2) + __shfl_down_sync(0xffffffffu, lv[1], 1) +
+                       __shfl_up_sync(0xffffffffu, lv[3], 1) + __shfl_up_sync(0xffffffffu, lv[4], 2);
+    if (lane >= 2 && lane <= 29 && c >= -2 && c <= b.nx + 3 && tot != 0.0) dst[base + c] += tot;
 }
 
 // boundary^T: the transpose of k_boundary. Each ghost's adjoint (after the

@@ -81,6 +81,8 @@ struct cumc_ctx {
     MixedBufs mb{};
     MixedParams mp{};
     double* const* tape = nullptr;  // adjoint: 3 x 8 arrays receiving each stage's combine output
+    void* adj_slab = nullptr;       // adjoint scratch, kept between runs
+    size_t adj_slab_bytes = 0;
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];
@@ -694,6 +696,7 @@ int cumc_free(cumc_ctx* c) {
     for (auto& pe : c->prof) { cudaEventDestroy(pe.a); cudaEventDestroy(pe.b); }
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     for (void* p : c->allocs) cudaFree(p);
+    if (c->adj_slab) cudaFree(c->adj_slab);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -994,24 +997,20 @@ int cumc_launch_count(cumc_ctx* c, long long* count) {
 // ---------------------------------------------------------------------------
 namespace {
 
-// device scratch of one adjoint run, released on every return path
+// device scratch of an adjoint run: bump allocation from the context's
+// slab (one cudaMalloc, kept for later runs of the same or smaller size)
 struct AdjMem {
-    std::vector<void*> v;
-    ~AdjMem() {
-        for (void* p : v) cudaFree(p);
-    }
+    char* base = nullptr;
+    size_t cap = 0, off = 0;
 };
+constexpr size_t ADJ_ALIGN = 256;
+size_t adj_round(size_t b) { return (b + ADJ_ALIGN - 1) / ADJ_ALIGN * ADJ_ALIGN; }
 
 int adj_alloc(cumc_ctx* c, AdjMem& m, double** p, size_t n) {
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, n * sizeof(double));
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return c->fail(CUMC_ERR_NOMEM, "adjoint: cudaMalloc of %zu bytes failed: %s", n * sizeof(double),
-                       cudaGetErrorString(e));
-    }
-    m.v.push_back(q);
-    *p = static_cast<double*>(q);
+    const size_t b = adj_round(n * sizeof(double));
+    if (m.off + b > m.cap) return c->fail(CUMC_ERR_NOMEM, "adjoint: scratch slab too small (internal sizing error)");
+    *p = reinterpret_cast<double*>(m.base + m.off);
+    m.off += b;
     return CUMC_OK;
 }
 
@@ -1076,13 +1075,23 @@ Arr3 arr3(double* const* p) {
 }
 
 template <int RECON>
-void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, const AdjPrim& lp, double* const* lbf) {
-    const long long nx = (long long)(b.nx + 1) * (b.ny + 2) * (b.nz + 2);
-    const long long ny = (long long)(b.nx + 2) * (b.ny + 1) * (b.nz + 2);
-    const long long nz = (long long)(b.nx + 2) * (b.ny + 2) * (b.nz + 1);
-    launch(c, -1, nx, 128, k_adj_sweep<0, RECON>, b, c->tabs, pr, c->ggas, st, lp, lbf[0]);
-    launch(c, -1, ny, 128, k_adj_sweep<1, RECON>, b, c->tabs, pr, c->ggas, st, lp, lbf[1]);
-    launch(c, -1, nz, 128, k_adj_sweep<2, RECON>, b, c->tabs, pr, c->ggas, st, lp, lbf[2]);
+void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, const AdjPrim& lp, double* const* lbf,
+                const FaceAdj& fa) {
+    const long long fx = (long long)(b.nx + 1) * (b.ny + 2) * (b.nz + 2);
+    const long long fy = (long long)(b.nx + 2) * (b.ny + 1) * (b.nz + 2);
+    const long long fz = (long long)(b.nx + 2) * (b.ny + 2) * (b.nz + 1);
+    // x: pass A per face, pass B one lane per cell (28 owned cells a warp)
+    launch(c, -1, fx, 128, k_adj_hll<0, RECON>, b, c->tabs, pr, c->ggas, st, fa, lbf[0]);
+    const long long xwarps = (long long)(b.ny + 2) * (b.nz + 2) * ((b.nx + 6 + 27) / 28);
+    launch_grid(c, -1, dim3((unsigned)((xwarps * 32 + 127) / 128), 7), 128, 0, k_adj_recon_x<RECON>, b, c->tabs, pr, fa,
+                lp);
+    // y, z: pass A per face, pass B one thread per (column, field)
+    launch(c, -1, fy, 128, k_adj_hll<1, RECON>, b, c->tabs, pr, c->ggas, st, fa, lbf[1]);
+    launch_grid(c, -1, dim3((unsigned)((WalkGeom<1>::ncols(b) + 127) / 128), 7, (b.ny + 2 + RC_SEG - 1) / RC_SEG), 128,
+                0, k_adj_recon_col<1, RECON>, b, c->tabs, pr, fa, lp);
+    launch(c, -1, fz, 128, k_adj_hll<2, RECON>, b, c->tabs, pr, c->ggas, st, fa, lbf[2]);
+    launch_grid(c, -1, dim3((unsigned)((WalkGeom<2>::ncols(b) + 127) / 128), 7, (b.nz + 2 + RC_SEG - 1) / RC_SEG), 128,
+                0, k_adj_recon_col<2, RECON>, b, c->tabs, pr, fa, lp);
 }
 
 template <bool FROM_CONS>
@@ -1101,15 +1110,33 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
     const size_t NT = (size_t)b.count();
     const size_t bytes = NT * sizeof(double);
     const int nck = (N + K - 1) / K;
-    const size_t arrays = (size_t)nck * STATE_ARRAYS + (size_t)K * 24 + 3 * STATE_ARRAYS + 8 * 3 + 3 * 2 + 9;
-    {
+    const size_t arrays = (size_t)nck * STATE_ARRAYS + (size_t)K * 24 + 3 * STATE_ARRAYS + 8 * 3 + 3 * 2 + 9 + 14;
+    const long long ncell = (long long)b.nx * b.ny * b.nz;
+    const int nblk = (int)((ncell + 255) / 256);
+    const size_t need = arrays * adj_round(bytes) + adj_round((size_t)(nblk + 1) * sizeof(double)) +
+                        adj_round((size_t)N * sizeof(double));
+    if (c->adj_slab_bytes < need) {
+        if (c->adj_slab) {
+            CUMC_CHECK(cudaStreamSynchronize(c->stream));
+            cudaFree(c->adj_slab);
+            c->adj_slab = nullptr;
+            c->adj_slab_bytes = 0;
+        }
         size_t fr = 0, tot = 0;
         CUMC_CHECK(cudaMemGetInfo(&fr, &tot));
-        if (arrays * bytes + (256u << 20) > fr)
+        if (need + (256u << 20) > fr)
             return c->fail(CUMC_ERR_NOMEM, "adjoint needs %.2f GB of device memory (%zu arrays), %.2f GB free",
-                           arrays * bytes / 1e9, arrays, fr / 1e9);
+                           need / 1e9, arrays, fr / 1e9);
+        if (cudaMalloc(&c->adj_slab, need) != cudaSuccess) {
+            cudaGetLastError();
+            c->adj_slab = nullptr;
+            return c->fail(CUMC_ERR_NOMEM, "adjoint: cudaMalloc of %.2f GB failed", need / 1e9);
+        }
+        c->adj_slab_bytes = need;
     }
     AdjMem m;
+    m.base = static_cast<char*>(c->adj_slab);
+    m.cap = c->adj_slab_bytes;
     int rc;
     std::vector<StateSet> ck(nck);
     for (auto& s : ck)
@@ -1133,8 +1160,10 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
     for (int q = 0; q < 3; ++q)
         if ((rc = adj_alloc(c, m, &lp.bc[q], NT)) != CUMC_OK) return rc;
     if ((rc = adj_alloc(c, m, &lp.eps, NT)) != CUMC_OK) return rc;
-    const long long ncell = (long long)b.nx * b.ny * b.nz;
-    const int nblk = (int)((ncell + 255) / 256);
+    FaceAdj fa;
+    for (int q = 0; q < 7; ++q)
+        if ((rc = adj_alloc(c, m, &fa.l[q], NT)) != CUMC_OK || (rc = adj_alloc(c, m, &fa.r[q], NT)) != CUMC_OK)
+            return rc;
     double *partial, *ddt;
     if ((rc = adj_alloc(c, m, &partial, (size_t)nblk + 1)) != CUMC_OK) return rc;
     if ((rc = adj_alloc(c, m, &ddt, (size_t)N)) != CUMC_OK) return rc;
@@ -1239,8 +1268,8 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
                 launch(c, -1, (long long)(b.nx + 2) * (b.ny + 2) * (b.nz + 2), 256, k_adj_ecell, b, pr,
                        (const double*)lamE[0], (const double*)lamE[1], (const double*)lamE[2], lp);
                 double* const* lbf = s >= 2 ? lamCur + IBX : lamU0 + IBX;
-                if (c->recon == CUMC_PPMC) adj_sweeps<4>(c, b, pr, st, lp, lbf);
-                else adj_sweeps<1>(c, b, pr, st, lp, lbf);
+                if (c->recon == CUMC_PPMC) adj_sweeps<4>(c, b, pr, st, lp, lbf, fa);
+                else adj_sweeps<1>(c, b, pr, st, lp, lbf, fa);
                 pc = 1 - pc;
             }
             std::swap(lamCur, lamU0);  // adjoint of the step's starting state

@@ -189,7 +189,7 @@ int cumc_launch_count(cumc_ctx* ctx, long long* count);
  * dt_out (may be NULL). Memory is traded for recomputation: the forward state
  * is checkpointed every checkpoint_every steps and each segment is recomputed
  * once during the reverse sweep; this needs
- *   (ceil(nsteps/checkpoint_every) * 17 + checkpoint_every * 24 + 93)
+ *   (ceil(nsteps/checkpoint_every) * 17 + checkpoint_every * 24 + 107)
  * arrays of (nx+6)(ny+6)(nz+6) doubles of device memory (CUMC_ERR_NOMEM if
  * absent).
  *
