@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -232,6 +234,92 @@ def run_reference(args, world, rank):
 
 
 # ---------------------------------------------------------------------------
+def mixed_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> dict:
+    """The mixed form (CUMC_MIXED) on the same workload: throughput, its ratio
+    to the FP64 path, and its relative L1 error per conserved variable and
+    normalised max |div B| against the FP64 path (bit-identical to the FP64
+    oracle) at t = 0.05, for B as given and B x 10 (plasma beta ~0.05)."""
+    import torch
+    from cumpic_b200 import _native as NN
+    from cumpic_b200 import problems as P
+    from cumpic_b200.solver import CUMC3D
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from compare import rel_l1_interior
+
+    prob = P.orszag_tang(n, precision=NN.MIXED)
+    sim = CUMC3D(prob)
+    sim.upload()
+    sim.initial_update()
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    sim.advance(warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.advance(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    sim.close()
+    out = {"value": prob.cells * steps / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms / steps,
+           "speedup_vs_fp64": fp64_ms_per_step / (ms / steps), "accuracy_t": 0.05, "vs_fp64": {}}
+    names = ("rho", "mx", "my", "mz", "E", "bx", "by", "bz")
+    for bscale in (1.0, 10.0):
+        res = {}
+        for prec in (NN.FP64, NN.MIXED):
+            s = CUMC3D(P.orszag_tang(n, bscale=bscale, precision=prec))
+            s.upload()
+            s.initial_update()
+            s.run(0.05)
+            res[prec] = (s.download(), s.find_divb()[1])
+            s.close()
+        rel = rel_l1_interior(res[NN.MIXED][0], res[NN.FP64][0])
+        out["vs_fp64"][f"bscale_{bscale:g}"] = {"rel_l1": {k: rel[q] for q, k in enumerate(names)},
+                                                "max_divb_norm": res[NN.MIXED][1]}
+    return out
+
+
+def adjoint_section(n: int = 128, steps: int = 200, ckpt: int = 20) -> dict:
+    """Cost of the discrete adjoint on the adjoint check configuration
+    (periodic box, rho = p = 1, uniform B, smooth velocity modes): the wall
+    time of cumc_adjoint_run (checkpointed forward pass, recomputation,
+    reverse sweep) over that of the same forward run with the same dt."""
+    import torch
+    from cumpic_b200 import _native as NN
+    from cumpic_b200 import problems as P
+    from cumpic_b200.solver import CUMC3D
+
+    prob = P.fourier_box(n)
+    sim = CUMC3D(prob)
+    sim.upload()
+    dts = sim.adjoint(steps, ckpt, NN.OBJ_MAGNETIC)["dts"]  # warm-up; records dt
+    fw = CUMC3D(prob)
+    fw.upload()
+    fw.initial_update()
+    for dt in dts[:5]:
+        fw.rungekutta(dt)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fw.upload()
+    fw.initial_update()
+    for dt in dts:
+        fw.rungekutta(dt)
+    fw.find_divb()  # synchronises
+    t_fwd = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.upload()
+    r = sim.adjoint(steps, ckpt, NN.OBJ_MAGNETIC, dts=dts)
+    t_adj = time.perf_counter() - t0
+    fw.close()
+    sim.close()
+    return {"workload": f"fourier_box n={n} steps={steps} checkpoint_every={ckpt} objective=magnetic_energy",
+            "forward_s": t_fwd, "adjoint_s": t_adj, "cost_ratio": t_adj / t_fwd, "J": r["J"],
+            "what": "adjoint_s: cumc_adjoint_run (initial_update, checkpointed forward pass, one recomputation "
+                    "of every segment but the last, reverse sweep, gradient download); forward_s: upload, "
+                    "initial_update and the same steps with the same dt"}
+
+
+# ---------------------------------------------------------------------------
 def run_ours(args, world, rank, local):
     import torch
     import numpy as np
@@ -361,6 +449,10 @@ def run_ours(args, world, rank, local):
                                 "sample": f"Orszag-Tang {n}x{n}x{nz} slab at cell size 1/{n}, 2 RK3 steps after 1 "
                                           f"warm-up ({el:.1f} s; FP64 C++ restatement, OpenMP)"}
     sim.close()
+    if world == 1 and not args.no_mixed:
+        line["mixed"] = mixed_section(n, args.steps, args.warmup, ms_max / args.steps)
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_section()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -46,29 +46,34 @@ struct AdjPrim {
 // reconstruction transposes (branches frozen by recomputation)
 // ---------------------------------------------------------------------------
 
-// d slope / d(vm, vc, vp) of ppm_slope, times lam, added to l[0..2]
-__device__ __forceinline__ void ppm_slope_adj(double vm, double vc, double vp, double b0, double b1, double lam,
-                                              double& lm, double& lc, double& lp) {
-    if (lam == 0.0) return;
+// ppm_slope's value (bit-identical: the same expression) and its partial
+// derivatives with respect to (vm, vc, vp), on the branch the value took
+struct SlopeGrad {
+    double d, gm, gc, gp;
+};
+__device__ __forceinline__ SlopeGrad ppm_slope_grad(double vm, double vc, double vp, double b0, double b1) {
+    SlopeGrad s{0.0, 0.0, 0.0, 0.0};
     const double delta = b0 * (vp - vc) + b1 * (vc - vm);
-    if (!((vp - vc) * (vc - vm) > 0.0)) return;
-    const double m1 = fabs(delta), m2 = 2.0 * fabs(vc - vm), m3 = 2.0 * fabs(vc - vp);
-    const double sd = copysign(1.0, delta);
-    const double m12 = fmin(m1, m2);
-    const int sel = m12 <= m3 ? (m1 <= m2 ? 1 : 2) : 3;
-    if (sel == 1) {  // slope = delta
-        lp += b0 * lam;
-        lc += (b1 - b0) * lam;
-        lm -= b1 * lam;
-    } else if (sel == 2) {  // slope = sd * 2 |vc - vm|
-        const double g = sd * 2.0 * copysign(1.0, vc - vm) * lam;
-        lc += g;
-        lm -= g;
-    } else {  // slope = sd * 2 |vc - vp|
-        const double g = sd * 2.0 * copysign(1.0, vc - vp) * lam;
-        lc += g;
-        lp -= g;
+    if ((vp - vc) * (vc - vm) > 0.0) {
+        const double m1 = fabs(delta), m2 = 2.0 * fabs(vc - vm), m3 = 2.0 * fabs(vc - vp);
+        const double sd = copysign(1.0, delta);
+        const double m12 = fmin(m1, m2);
+        s.d = fmin(m12, m3) * sd;
+        if (m12 <= m3 && m1 <= m2) {  // slope = delta
+            s.gm = -b1;
+            s.gc = b1 - b0;
+            s.gp = b0;
+        } else if (m12 <= m3) {  // slope = sd 2 |vc - vm|
+            const double g = sd * 2.0 * copysign(1.0, vc - vm);
+            s.gm = -g;
+            s.gc = g;
+        } else {  // slope = sd 2 |vc - vp|
+            const double g = sd * 2.0 * copysign(1.0, vc - vp);
+            s.gc = g;
+            s.gp = -g;
+        }
     }
+    return s;
 }
 
 // transpose of the reconstruction of one cell from v[0..4] = cells c-2..c+2:
@@ -78,9 +83,10 @@ __device__ __forceinline__ void recon_adj(const AxisTabs& A, int c, const double
                                           double lv[5]) {
     if (lvm == 0.0 && lvp == 0.0) return;
     if (RECON == 4) {
-        const double dmm = ppm_slope(v[0], v[1], v[2], A.s0[c - 1], A.s1[c - 1]);
-        const double dmc = ppm_slope(v[1], v[2], v[3], A.s0[c], A.s1[c]);
-        const double dmp = ppm_slope(v[2], v[3], v[4], A.s0[c + 1], A.s1[c + 1]);
+        const SlopeGrad sm = ppm_slope_grad(v[0], v[1], v[2], A.s0[c - 1], A.s1[c - 1]);
+        const SlopeGrad sc = ppm_slope_grad(v[1], v[2], v[3], A.s0[c], A.s1[c]);
+        const SlopeGrad sp = ppm_slope_grad(v[2], v[3], v[4], A.s0[c + 1], A.s1[c + 1]);
+        const double dmm = sm.d, dmc = sc.d, dmp = sp.d;
         const double vl = ppm_face(v[1], v[2], dmm, dmc, A.a0[c - 1], A.a1[c - 1], A.a2[c - 1], A.a3[c - 1]);
         const double vr = ppm_face(v[2], v[3], dmc, dmp, A.a0[c], A.a1[c], A.a2[c], A.a3[c]);
         const double vc = v[2];
@@ -121,9 +127,11 @@ __device__ __forceinline__ void recon_adj(const AxisTabs& A, int c, const double
             ldmc += A.a3[c] * lvr;
         }
         lv[2] += lvc;
-        ppm_slope_adj(v[0], v[1], v[2], A.s0[c - 1], A.s1[c - 1], ldmm, lv[0], lv[1], lv[2]);
-        ppm_slope_adj(v[1], v[2], v[3], A.s0[c], A.s1[c], ldmc, lv[1], lv[2], lv[3]);
-        ppm_slope_adj(v[2], v[3], v[4], A.s0[c + 1], A.s1[c + 1], ldmp, lv[2], lv[3], lv[4]);
+        lv[0] += ldmm * sm.gm;
+        lv[1] += ldmm * sm.gc + ldmc * sc.gm;
+        lv[2] += ldmm * sm.gp + ldmc * sc.gc + ldmp * sp.gm;
+        lv[3] += ldmc * sc.gp + ldmp * sp.gc;
+        lv[4] += ldmp * sp.gp;
     } else {
         // vm = vc - sl/2, vp = vc + sl/2, sl = minmod of dqf = 2(vp-vc)/cf, dqb = 2(vc-vm)/cb
         lv[2] += lvm + lvp;
@@ -627,27 +635,31 @@ __global__ void __launch_bounds__(128) k_adj_recon_x(Box b, Tabs T, Prim pr, Fac
     const int lane = threadIdx.x & 31;
     const long long rows = (long long)(b.ny + 2) * (b.nz + 2);
     if (warp >= rows * nw) return;  // whole warp
-    const int v = blockIdx.y;
     const int w = (int)(warp % nw);
     const long long row = warp / nw;
     const int k = (int)(row % (b.ny + 2)), l = (int)(row / (b.ny + 2));
     const int c = 28 * w + lane - 4;
     const AxisTabs A = T.ax[0];
-    const double* src;
-    double* dst;
-    sweep_field<0>(pr, o, v, src, dst);
     const int base = b.idx(0, k, l);
-    double lv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (c >= 0 && c <= b.nx + 1) {
-        const double* q = src + base + c;
-        const double x[5] = {q[-2], q[-1], q[0], q[1], q[2]};
-        const double lvm = c >= 1 ? fa.r[v][base + c - 1] : 0.0;
-        const double lvp = c <= b.nx ? fa.l[v][base + c] : 0.0;
-        recon_adj<RECON>(A, c, x, lvm, lvp, lv);
+    const bool mine = c >= 0 && c <= b.nx + 1;                  // a reconstructed cell
+    const bool owned = lane >= 2 && lane <= 29 && c >= -2 && c <= b.nx + 3;
+#pragma unroll 1
+    for (int v = 0; v < 7; ++v) {
+        const double* src;
+        double* dst;
+        sweep_field<0>(pr, o, v, src, dst);
+        double lv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        if (mine) {
+            const double* q = src + base + c;
+            const double x[5] = {q[-2], q[-1], q[0], q[1], q[2]};
+            const double lvm = c >= 1 ? fa.r[v][base + c - 1] : 0.0;
+            const double lvp = c <= b.nx ? fa.l[v][base + c] : 0.0;
+            recon_adj<RECON>(A, c, x, lvm, lvp, lv);
+        }
+        const double tot = lv[2] + __shfl_down_sync(0xffffffffu, lv[0], 2) + __shfl_down_sync(0xffffffffu, lv[1], 1) +
+                           __shfl_up_sync(0xffffffffu, lv[3], 1) + __shfl_up_sync(0xffffffffu, lv[4], 2);
+        if (owned && tot != 0.0) dst[base + c] += tot;
     }
-    const double tot = lv[2] + __shfl_down_sync(0xffffffffu, lv[0], 2) + __shfl_down_sync(0xffffffffu, lv[1], 1) +
-                       __shfl_up_sync(0xffffffffu, lv[3], 1) + __shfl_up_sync(0xffffffffu, lv[4], 2);
-    if (lane >= 2 && lane <= 29 && c >= -2 && c <= b.nx + 3 && tot != 0.0) dst[base + c] += tot;
 }
 
 // boundary^T: the transpose of k_boundary. Each ghost's adjoint (after the
@@ -755,7 +767,8 @@ __global__ void __launch_bounds__(256) k_adj_boundary(Box b, BoundArgs fw, AdjPr
 // receives (rho, vx, vy, vz, eps) adjoints.
 template <int MODEL, bool FROM_CONS>
 __global__ void __launch_bounds__(256) k_adj_utop(Box b, Arr8 u, Arr8 w0, const double* eps0, Arr8 lu,
-                                                  AdjPrim o, double ggas, Arr8 mu, Arr3 lb) {
+                                                  AdjPrim o, double ggas, Arr8 mu, Arr3 lb, double alpha,
+                                                  double beta, Arr8 lam0) {
     const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
     const long long total = (long long)n0 * n1 * n2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -764,7 +777,10 @@ __global__ void __launch_bounds__(256) k_adj_utop(Box b, Arr8 u, Arr8 w0, const 
     const int i = b.idx(j, k, l);
     if (!(j >= 1 && k >= 1 && l >= 1)) {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) mu.a[q][i] = 0.0;
+        for (int q = 0; q < 5; ++q) {
+            mu.a[q][i] = 0.0;
+            if (beta != 0.0) lu.a[q][i] = 0.0;
+        }
 #pragma unroll
         for (int q = 0; q < 3; ++q) lb.a[q][i] = 0.0;
         return;
@@ -831,12 +847,23 @@ __global__ void __launch_bounds__(256) k_adj_utop(Box b, Arr8 u, Arr8 w0, const 
     lb.a[0][i] = o.bc[0][i] + 2.0 * bx * Lbsq;
     lb.a[1][i] = o.bc[1][i] + 2.0 * by * Lbsq;
     lb.a[2][i] = o.bc[2][i] + 2.0 * bz * Lbsq;
+    // combine^T of the hydro part: Upre = alpha U0 + beta U_prev + ...; the
+    // adjoint of U_prev replaces lu (read above by this thread only)
+    if (FROM_CONS && (alpha != 0.0 || beta != 0.0)) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double m = mu.a[q][i];
+            lam0.a[q][i] += alpha * m;
+            if (beta != 0.0) lu.a[q][i] = beta * m;
+        }
+    }
 }
 
 // face-field adjoint on (0:n)^3: the pass-through adjoint of the live face
 // values plus half the adjoints of the two active cells whose bcell average
 // reads the face (solver/fromrvetou.f90:97-107); zero on every other entry
-__global__ void __launch_bounds__(256) k_adj_bface(Box b, Arr3 lbf, Arr3 lb, Arr3 out) {
+__global__ void __launch_bounds__(256) k_adj_bface(Box b, Arr3 lbf, Arr3 lb, Arr3 out, double alpha, double beta,
+                                                   Arr3 lam0) {
     const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
     const long long total = (long long)n0 * n1 * n2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -860,20 +887,10 @@ __global__ void __launch_bounds__(256) k_adj_bface(Box b, Arr3 lbf, Arr3 lb, Arr
             v += 0.5 * (left + right);
         }
         out.a[d][i] = v;
-    }
-}
-
-// combine^T, elementwise over the box: lamU0 += a mu, lamCur = b mu (b = 0:
-// left alone). mu is zero off the live entries.
-__global__ void __launch_bounds__(256) k_adj_combine(long long n, Arr8 mu, double a, double bco, Arr8 lam0,
-                                                     Arr8 lamc) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const double m = mu.a[q][t];
-        lam0.a[q][t] += a * m;
-        if (bco != 0.0) lamc.a[q][t] = bco * m;
+        // combine^T of the field part (lbf, read above by this thread only,
+        // becomes the adjoint of the previous stage's face field)
+        if (alpha != 0.0) lam0.a[d][i] += alpha * v;
+        if (beta != 0.0) lbf.a[d][i] = beta * v;
     }
 }
 

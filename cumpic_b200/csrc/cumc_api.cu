@@ -1083,8 +1083,7 @@ void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, c
     // x: pass A per face, pass B one lane per cell (28 owned cells a warp)
     launch(c, -1, fx, 128, k_adj_hll<0, RECON>, b, c->tabs, pr, c->ggas, st, fa, lbf[0]);
     const long long xwarps = (long long)(b.ny + 2) * (b.nz + 2) * ((b.nx + 6 + 27) / 28);
-    launch_grid(c, -1, dim3((unsigned)((xwarps * 32 + 127) / 128), 7), 128, 0, k_adj_recon_x<RECON>, b, c->tabs, pr, fa,
-                lp);
+    launch(c, -1, xwarps * 32, 128, k_adj_recon_x<RECON>, b, c->tabs, pr, fa, lp);
     // y, z: pass A per face, pass B one thread per (column, field)
     launch(c, -1, fy, 128, k_adj_hll<1, RECON>, b, c->tabs, pr, c->ggas, st, fa, lbf[1]);
     launch_grid(c, -1, dim3((unsigned)((WalkGeom<1>::ncols(b) + 127) / 128), 7, (b.ny + 2 + RC_SEG - 1) / RC_SEG), 128,
@@ -1096,12 +1095,12 @@ void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, c
 
 template <bool FROM_CONS>
 void adj_utop(cumc_ctx* c, const Box& b, Arr8 u, Arr8 w0, const double* eps0, Arr8 lu, const AdjPrim& lp, Arr8 mu,
-              Arr3 lb) {
+              Arr3 lb, double alpha = 0.0, double beta = 0.0, Arr8 lam0 = Arr8{}) {
     const long long n = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
     if (c->model == CUMC_MODEL_RIEMANN)
-        launch(c, -1, n, 256, k_adj_utop<1, FROM_CONS>, b, u, w0, eps0, lu, lp, c->ggas, mu, lb);
+        launch(c, -1, n, 256, k_adj_utop<1, FROM_CONS>, b, u, w0, eps0, lu, lp, c->ggas, mu, lb, alpha, beta, lam0);
     else
-        launch(c, -1, n, 256, k_adj_utop<0, FROM_CONS>, b, u, w0, eps0, lu, lp, c->ggas, mu, lb);
+        launch(c, -1, n, 256, k_adj_utop<0, FROM_CONS>, b, u, w0, eps0, lu, lp, c->ggas, mu, lb, alpha, beta, lam0);
 }
 
 int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const double* dt_in, double* dt_out,
@@ -1182,8 +1181,10 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
     utop(c, b, c->U[c->cur], false);
     boundary(c, b, c->U[c->cur]);
     std::vector<double> dts((size_t)N);
+    const int last0 = (nck - 1) * K;  // the last segment is taped now, not recomputed
     for (int n = 0; n < N; ++n) {
         if (n % K == 0) copy_state(c, ck[n / K], live_state(c));
+        c->tape = n >= last0 ? &tape[(size_t)(n - last0) * 24] : nullptr;
         double dt;
         if (dt_in) {
             dt = dt_in[n];
@@ -1197,6 +1198,7 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
         launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
         rk_step(c, b);
     }
+    c->tape = nullptr;
     copy_state(c, fin, live_state(c));
     CUMC_CHECK(cudaMemcpyAsync(c->host_pinned + 1, c->flag_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
     CUMC_CHECK(cudaStreamSynchronize(c->stream));
@@ -1229,13 +1231,15 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
     bool have_next = false;  // P[pc] holds the primitives after step n
     for (int seg = nck - 1; seg >= 0; --seg) {
         const int a0 = seg * K, a1 = std::min(N, a0 + K);
-        copy_state(c, live_state(c), ck[seg]);
-        for (int n = a0; n < a1; ++n) {
-            c->tape = &tape[(size_t)(n - a0) * 24];
-            launch(c, -1, 1, 1, k_set_scalar, c->scal, dts[n]);
-            rk_step(c, b);
+        if (seg != nck - 1) {  // recompute the segment, taping each stage
+            copy_state(c, live_state(c), ck[seg]);
+            for (int n = a0; n < a1; ++n) {
+                c->tape = &tape[(size_t)(n - a0) * 24];
+                launch(c, -1, 1, 1, k_set_scalar, c->scal, dts[n]);
+                rk_step(c, b);
+            }
+            c->tape = nullptr;
         }
-        c->tape = nullptr;
         for (int n = a1 - 1; n >= a0; --n) {
             double* const* tp = &tape[(size_t)(n - a0) * 24];
             if (!have_next) adj_prims_from(c, b, tp + 16, P[pc]);
@@ -1249,12 +1253,11 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
                 // boundary^T and utop^T of the stage's output
                 launch(c, -1, ghost_count(b), 256, k_adj_boundary, b, bound_args(c, Pc.u, Pc.prim()), lp,
                        lamCur[IBX], lamCur[IBY], lamCur[IBZ]);
-                adj_utop<true>(c, b, arr8(tp + (s - 1) * 8), arr8(Pc.w, 5), nullptr, arr8(lamCur), lp, arr8(mu), arr3(lb));
+                // utop^T and the face-field gather, each with the combine^T of its part
+                adj_utop<true>(c, b, arr8(tp + (s - 1) * 8), arr8(Pc.w, 5), nullptr, arr8(lamCur), lp, arr8(mu), arr3(lb),
+                               alpha[s], beta[s], arr8(lamU0));
                 launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_bface, b, arr3(lamCur + IBX),
-                       arr3(lb), arr3(mu + IBX));
-                // combine^T
-                launch(c, -1, (long long)NT, 256, k_adj_combine, (long long)NT, arr8(mu), alpha[s], beta[s],
-                       arr8(lamU0), arr8(lamCur));
+                       arr3(lb), arr3(mu + IBX), alpha[s], beta[s], arr3(lamU0 + IBX));
                 zero_lp();
                 // L^T at the stage's input
                 AdjStage st;
@@ -1281,7 +1284,7 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
            lamCur[IBY], lamCur[IBZ]);
     adj_utop<false>(c, b, arr8(ck[0].u), arr8(ck[0].w, 5), ck[0].eps, arr8(lamCur), lp, arr8(mu), arr3(lb));
     launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_bface, b, arr3(lamCur + IBX), arr3(lb),
-           arr3(mu + IBX));
+           arr3(mu + IBX), 0.0, 0.0, Arr3{});
     if ((rc = sync_status(c)) != CUMC_OK) return rc;
     if (grad_prim) {
         const double* s[8] = {mu[0], mu[1], mu[2], mu[3], nullptr, mu[IBX], mu[IBY], mu[IBZ]};
