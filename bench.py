@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-check", action="store_true",
+                    help="also run the full finite-difference check of the adjoint (128^3, 200 steps, 16 directions)")
+    ap.add_argument("--all-configs", action="store_true",
+                    help="also run Orszag-Tang 512^3 (mixed vs FP64) and the torus over 2000 steps (FP64, mixed)")
     return ap.parse_args()
 
 
@@ -313,10 +317,120 @@ def adjoint_section(n: int = 128, steps: int = 200, ckpt: int = 20) -> dict:
     fw.close()
     sim.close()
     return {"workload": f"fourier_box n={n} steps={steps} checkpoint_every={ckpt} objective=magnetic_energy",
-            "forward_s": t_fwd, "adjoint_s": t_adj, "cost_ratio": t_adj / t_fwd, "J": r["J"],
+            "forward_s": t_fwd, "adjoint_s": t_adj, "cost_ratio": t_adj / t_fwd,
+            "cost_ratio_beyond_forward": (t_adj - t_fwd) / t_fwd, "J": r["J"],
             "what": "adjoint_s: cumc_adjoint_run (initial_update, checkpointed forward pass, one recomputation "
                     "of every segment but the last, reverse sweep, gradient download); forward_s: upload, "
                     "initial_update and the same steps with the same dt"}
+
+
+def config_runs() -> dict:
+    """The remaining configurations: Orszag-Tang 512^3 in the mixed form
+    against FP64 (t = 0.05), and the spherical torus 192 x 128 x 64 over 2000
+    steps in FP64 and in the mixed form (throughput, the mixed run's relative
+    L1 against the FP64 run, both runs' normalised max |div B|)."""
+    import torch
+    from cumpic_b200 import _native as NN
+    from cumpic_b200 import problems as P
+    from cumpic_b200.solver import CUMC3D
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from compare import rel_l1_interior
+    names = ("rho", "mx", "my", "mz", "E", "bx", "by", "bz")
+
+    def timed(sim, fn):
+        stream = torch.cuda.ExternalStream(sim.stream_handle())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    out = {}
+    res = {}
+    for prec in (NN.FP64, NN.MIXED):
+        prob = P.orszag_tang(512, precision=prec)
+        s = CUMC3D(prob)
+        s.upload()
+        s.initial_update()
+        ms = timed(s, lambda: s.run(0.05))
+        res[prec] = (s.download(), s.find_divb()[1], prob.cells * s.n_step / (ms / 1e3) / 1e6, s.n_step)
+        s.close()
+    rel = rel_l1_interior(res[NN.MIXED][0], res[NN.FP64][0])
+    out["orszag_tang_512_t0.05"] = {
+        "fp64_mcell_upd_s": res[NN.FP64][2], "mixed_mcell_upd_s": res[NN.MIXED][2],
+        "steps": {"fp64": res[NN.FP64][3], "mixed": res[NN.MIXED][3]},
+        "mixed_rel_l1_vs_fp64": {k: rel[q] for q, k in enumerate(names)},
+        "max_divb_norm": {"fp64": res[NN.FP64][1], "mixed": res[NN.MIXED][1]}}
+    # torus: throughput with the device-side dt, then the accuracy runs with
+    # the FP64 run's dt sequence replayed by the mixed run (same times)
+    rate = {}
+    for prec in (NN.FP64, NN.MIXED):
+        prob = P.torus()
+        prob.precision = prec
+        s = CUMC3D(prob)
+        s.upload()
+        s.initial_update()
+        ms = timed(s, lambda: s.advance(2000))
+        rate[prec] = prob.cells * 2000 / (ms / 1e3) / 1e6
+        s.close()
+    res = {}
+    dts = []
+    for prec in (NN.FP64, NN.MIXED):
+        prob = P.torus()
+        prob.precision = prec
+        s = CUMC3D(prob)
+        s.upload()
+        s.initial_update()
+        for n in range(2000):
+            if prec == NN.FP64:
+                dts.append(s.finddt())
+            s.rungekutta(dts[n])
+        res[prec] = (s.download(), s.find_divb()[1])
+        s.close()
+    rel = rel_l1_interior(res[NN.MIXED][0], res[NN.FP64][0])
+    out["torus_192x128x64_2000_steps"] = {
+        "fp64_mcell_upd_s": rate[NN.FP64], "mixed_mcell_upd_s": rate[NN.MIXED], "t_end": float(sum(dts)),
+        "mixed_rel_l1_vs_fp64": {k: rel[q] for q, k in enumerate(names)},
+        "max_divb_norm": {"fp64": res[NN.FP64][1], "mixed": res[NN.MIXED][1]},
+        "accuracy_runs": "both with the FP64 run's 2000 dt values"}
+    return out
+
+
+def adjoint_check(n: int = 128, steps: int = 200, ckpt: int = 20, ndir: int = 16, eps: float = 1e-6) -> dict:
+    """The adjoint check configuration in full: gradient of the final magnetic
+    energy with respect to the initial velocity against central differences
+    (step eps relative to the flow) along `ndir` seeded smooth random
+    directions, with the adjoint's dt sequence replayed."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from cumpic_b200 import _native as NN
+    from cumpic_b200 import problems as P
+    from cumpic_b200.solver import CUMC3D
+    from test_gpu_adjoint import _density, smooth_velocity_directions
+
+    prob = P.fourier_box(n)
+    sim = CUMC3D(prob)
+    sim.upload()
+    res = sim.adjoint(steps, ckpt, NN.OBJ_MAGNETIC)
+    fw = CUMC3D(prob)
+
+    def run(prim):
+        fw.upload(prim, prob.eps)
+        fw.initial_update()
+        for dt in res["dts"]:
+            fw.rungekutta(dt)
+        return _density(fw.download(), prob, NN.OBJ_MAGNETIC)
+
+    rels = []
+    for dp, _ in smooth_velocity_directions(prob, ndir, 4):
+        fd = float(np.sum(run(prob.prim + eps * dp) - run(prob.prim - eps * dp))) / (2 * eps)
+        ad = float(np.sum(res["grad_prim"] * dp))
+        rels.append(abs(fd - ad) / max(abs(fd), abs(ad)))
+    return {"workload": f"fourier_box n={n} steps={steps} checkpoint_every={ckpt}", "directions": ndir,
+            "eps_relative": eps, "max_rel_err": max(rels), "median_rel_err": statistics.median(rels),
+            "rel_errs": rels}
 
 
 # ---------------------------------------------------------------------------
@@ -453,6 +567,10 @@ def run_ours(args, world, rank, local):
         line["mixed"] = mixed_section(n, args.steps, args.warmup, ms_max / args.steps)
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_section()
+        if args.adjoint_check:
+            line["adjoint"]["fd_check"] = adjoint_check()
+    if world == 1 and args.all_configs:
+        line["configs"] = config_runs()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

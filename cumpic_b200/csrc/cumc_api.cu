@@ -71,11 +71,13 @@ struct cumc_ctx {
     double graph_t_end = 0.0;
     long long graph_launches_per_step = 0;
     // sweep kernels (environment variable CUMC_SWEEP, for A/B timing; all
-    // give the same bits): 0 default (per-face x, shared-memory-window walker
-    // y/z), 1 "simple" (per-face everywhere), 2 "tile" (shared-memory tiles),
+    // give the same bits): 0 default (lane-per-cell x, shared-memory-window
+    // walker y/z), 1 "simple" (per-face everywhere), 2 "tile" (shared-memory tiles),
     // 3 "walkx" (register walker everywhere, x staged through shared memory),
     // 4 "walksm" (shared-memory-window walker everywhere), 5 "walkreg"
-    // (per-face x, register walker y/z)
+    // (per-face x, register walker y/z), 6 "xwarp" (lane-per-cell x only;
+    // y/z one thread per face), 7 "xface" (per-face x, shared-memory-window
+    // walker y/z)
     int sweep_mode = 0;
     bool mixed = false;         // CUMC_MIXED: state and kernels of cumc_mixed.cu
     MixedBufs mb{};
@@ -206,16 +208,16 @@ template <int DIR>
 void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
     FaceFlux out;
     for (int q = 0; q < 7; ++q) out.f[q] = c->F[DIR][q];
-    // default: one thread per face along x, the shared-memory-window walker
-    // along y and z (the fastest pairing measured at 256^3)
-    const bool walk = (DIR > 0 && (c->sweep_mode == 0 || c->sweep_mode == 5)) || c->sweep_mode == 3 ||
-                      c->sweep_mode == 4;
+    // default: one lane per cell along x, the shared-memory-window walker
+    // along y and z
+    const bool walk = (DIR > 0 && (c->sweep_mode == 0 || c->sweep_mode == 5 || c->sweep_mode == 7)) ||
+                      c->sweep_mode == 3 || c->sweep_mode == 4;
     if (walk) {  // column walker
         int nseg;
         const int seg = walk_segment(WalkGeom<DIR>::nd(b) + 1, 64, &nseg);
         const dim3 grid((unsigned)((WalkGeom<DIR>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
         const int cls = CUMC_K_SWEEP_X + DIR;
-        if (c->sweep_mode == 4 || c->sweep_mode == 0) {
+        if (c->sweep_mode == 4 || c->sweep_mode == 0 || c->sweep_mode == 7) {
             const size_t sm = walk_smem<double>(DIR);
             if (c->recon == CUMC_PPMC)
                 launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 4, double>, b, c->tabs, pr, c->ggas, out, seg);
@@ -228,6 +230,13 @@ void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
             else
                 launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk<DIR, 1, double>, b, c->tabs, pr, c->ggas, out, seg);
         }
+        return;
+    }
+    if (DIR == 0 && (c->sweep_mode == 0 || c->sweep_mode == 6)) {  // x: one lane per cell
+        if (c->recon == CUMC_PPMC)
+            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b), 128, k_sweep_xwarp<4, double>, b, c->tabs, pr, c->ggas, out);
+        else
+            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b), 128, k_sweep_xwarp<1, double>, b, c->tabs, pr, c->ggas, out);
         return;
     }
     if (c->sweep_mode != 2) {  // one thread per face
@@ -560,6 +569,8 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
                         : std::strcmp(sw, "walkx") == 0  ? 3
                         : std::strcmp(sw, "walksm") == 0 ? 4
                         : std::strcmp(sw, "walkreg") == 0 ? 5
+                        : std::strcmp(sw, "xwarp") == 0   ? 6
+                        : std::strcmp(sw, "xface") == 0   ? 7
                                                           : 0;
     }
     if ((rc = sweep_attributes(c)) != CUMC_OK) return fail_init(rc);

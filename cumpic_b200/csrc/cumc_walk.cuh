@@ -370,3 +370,71 @@ __global__ void __launch_bounds__(WK_THREADS) k_sweep_walk_sm(Box b, Tabs T, Pri
 }
 
 }  // namespace cumc
+
+namespace cumc {
+
+// ---------------------------------------------------------------------------
+// x sweep with one lane per cell (GET_FLUXES x sweep, solver/spatial.f90:131-168).
+// A warp holds 32 consecutive cells x0 .. x0+31 of one row. Each lane forms
+// its own cell's limited slope, the interface value with the next cell and
+// the extremum fix once, taking the neighbours' values through warp shuffles
+// (the same expressions and operand order as the per-face kernel, so the
+// fluxes are bit-identical); lanes 2..28 then solve HLL at their faces. A
+// warp yields 27 faces; consecutive warps overlap by 5 cells. Loads and
+// stores are one 256-byte row segment per field.
+// ---------------------------------------------------------------------------
+constexpr int XW_FACES = 27;
+
+template <int RECON, typename R>
+__global__ void __launch_bounds__(128) k_sweep_xwarp(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int nw = (b.nx + 1 + XW_FACES - 1) / XW_FACES;  // warps per row
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long rows = (long long)(b.ny + 2) * (b.nz + 2);
+    if (warp >= rows * nw || (b.skip && *b.skip)) return;  // uniform over the warp
+    const int w = (int)(warp % nw);
+    const long long row = warp / nw;
+    const int k = (int)(row % (b.ny + 2)), l = (int)(row / (b.ny + 2));
+    const int c = w * XW_FACES - 2 + lane;  // this lane's cell; its face is c | c+1
+    const bool inb = c >= -2 && c <= b.nx + 3;
+    const int ct = min(max(c, -2), b.nx + 3);  // table index kept in range for spare lanes
+    const int base = b.idx(0, k, l);
+    const AxisTabs A = T.ax[0];
+    const R* src[7] = {pr.w[0], pr.w[1], pr.w[2], pr.w[3], pr.w[4], pr.bc[1], pr.bc[2]};
+    const int slot[7] = {IRHO, IVX, IVY, IVZ, ITAU, IBY, IBZ};
+    R wl[8], wr[8];
+#pragma unroll
+    for (int v = 0; v < 7; ++v) {
+        const R x = inb ? src[v][base + c] : R(0);
+        const R xm = __shfl_up_sync(FULL, x, 1), xp = __shfl_down_sync(FULL, x, 1);
+        R vm, vp;
+        if (RECON == 4) {
+            const R d = ppm_slope(xm, x, xp, (R)A.s0[ct], (R)A.s1[ct]);
+            const R dp = __shfl_down_sync(FULL, d, 1);
+            const R V = ppm_face(x, xp, d, dp, (R)A.a0[ct], (R)A.a1[ct], (R)A.a2[ct], (R)A.a3[ct]);  // c | c+1
+            const R Vm = __shfl_up_sync(FULL, V, 1);                                                // c-1 | c
+            ppm_fix(x, Vm, V, vm, vp);
+        } else {
+            const R sl = tvd_slope(xm, x, xp, (R)A.tcf[ct], (R)A.tcb[ct]);
+            vm = x - R(0.5) * sl;
+            vp = x + R(0.5) * sl;
+        }
+        wl[slot[v]] = vp;                             // vp_out of cell c
+        wr[slot[v]] = __shfl_down_sync(FULL, vm, 1);  // vm_out of cell c+1
+    }
+    if (lane < 2 || lane > 28 || c < 0 || c > b.nx) return;
+    const R bn = pr.bf[0][base + c];
+    wl[IBX] = bn;
+    wr[IBX] = bn;
+    R fx[7];
+    hll_flux7<0>(wl, wr, ggas, fx);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) out.f[i][base + c] = fx[i];
+}
+
+inline long long xwarp_threads(const Box& b) {
+    return (long long)(b.ny + 2) * (b.nz + 2) * ((b.nx + 1 + XW_FACES - 1) / XW_FACES) * 32;
+}
+
+}  // namespace cumc

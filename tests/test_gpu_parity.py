@@ -188,7 +188,7 @@ def test_nonfinite_state_is_reported(precision):
     assert e.value.code == N.CUMC_ERR_NONFINITE
 
 
-SWEEP_MODES = ["simple", "tile", "walkx", "walksm", "walkreg"]
+SWEEP_MODES = ["simple", "tile", "walkx", "walksm", "walkreg", "xwarp", "xface"]
 
 
 @pytest.mark.parametrize("mode", SWEEP_MODES)
