@@ -369,18 +369,20 @@ void sweep_mx(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>
               int recon) {
     FaceFluxT<float> out;
     for (int q = 0; q < 7; ++q) out.f[q] = m.F[DIR][q];
-    if (DIR > 0) {  // column walker along y or z
+    if (DIR > 0) {  // column walker along y or z, window in shared memory
         constexpr int D = DIR > 0 ? DIR : 1;
         int nseg;
         const int seg = walk_segment(WalkGeom<D>::nd(b) + 1, 64, &nseg);
         const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
-        if (recon == 4) run(L, DIR, grid, WK_THREADS, 0, k_sweep_walk<D, 4, float>, b, T, pr, ggas, out, seg);
-        else run(L, DIR, grid, WK_THREADS, 0, k_sweep_walk<D, 1, float>, b, T, pr, ggas, out, seg);
+        const size_t sm = walk_smem<float>(D);
+        if (recon == 4) run(L, DIR, grid, WK_THREADS, sm, k_sweep_walk_sm<D, 4, float>, b, T, pr, ggas, out, seg);
+        else run(L, DIR, grid, WK_THREADS, sm, k_sweep_walk_sm<D, 1, float>, b, T, pr, ggas, out, seg);
         return;
     }
-    const long long n = (long long)(b.nx + 1) * (b.ny + 2) * (b.nz + 2);
-    if (recon == 4) run(L, DIR, g1(n, 128), 128, 0, k_sweep<0, 4, float>, b, T, pr, ggas, out);
-    else run(L, DIR, g1(n, 128), 128, 0, k_sweep<0, 1, float>, b, T, pr, ggas, out);
+    // x: one lane per cell
+    const long long n = xwarp_threads(b);
+    if (recon == 4) run(L, DIR, g1(n, 128), 128, 0, k_sweep_xwarp<4, float>, b, T, pr, ggas, out);
+    else run(L, DIR, g1(n, 128), 128, 0, k_sweep_xwarp<1, float>, b, T, pr, ggas, out);
 }
 
 UtopMx utop_args(const MixedBufs& m, const MixedParams& p) {
