@@ -119,8 +119,11 @@ def algorithmic_bytes(kernel: str, nx: int, ny: int, nz: int) -> float:
     box2 = (nx + 2) * (ny + 2) * (nz + 2)
     if kernel == "emf":
         return 8.0 * (6 * box2 + 6 * box2 + 3 * box1)
-    if kernel == "combine":  # 15 hydro fluxes + 3 EMF + u0 + uc + result (stage 2/3 form)
-        return 8.0 * (15 + 3 + 8 + 8 + 8) * box1
+    if kernel == "combine":  # hydro combine + conversions, stage 2/3 form: 15 hydro fluxes, u0 and uc
+        # hydro, 3 face fields in; hydro cons, w, bcell, eps out
+        return 8.0 * (15 + 5 + 5 + 3 + 5 + 5 + 3 + 1) * box1
+    if kernel == "ct":  # 3 EMF, u0 and uc face fields in, face fields out (stage 2/3 form)
+        return 8.0 * (3 + 3 + 3 + 3) * box1
     if kernel == "utop":
         return 8.0 * (8 + 2 + 5 + 5 + 1 + 3) * box1
     if kernel == "boundary":

@@ -32,7 +32,7 @@ MODEL_NONE, MODEL_RIEMANN, MODEL_TORUS_SPH, MODEL_TORUS_CYN = 0, 1, 2, 3
 OBJ_MAGNETIC, OBJ_KINETIC, OBJ_LINEAR = 1, 2, 3
 
 K_SWEEP_X, K_SWEEP_Y, K_SWEEP_Z, K_EMF, K_COMBINE, K_UTOP, K_BOUNDARY, K_FINDDT = range(8)
-K_NAMES = ["sweep_x", "sweep_y", "sweep_z", "emf", "combine", "utop", "boundary", "finddt"]
+K_NAMES = ["sweep_x", "sweep_y", "sweep_z", "emf", "combine", "utop", "boundary", "finddt", "ct"]
 
 
 class CumcConfig(ctypes.Structure):

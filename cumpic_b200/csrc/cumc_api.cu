@@ -266,27 +266,6 @@ int sweep_attributes(cumc_ctx* c) {
     return CUMC_OK;
 }
 
-template <int COORD, int MODEL>
-void combine_dispatch(cumc_ctx* c, const Box& b, int stage, const Prim& pr, const FaceFlux* ff, const CombineArgs& a) {
-    const long long n = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
-    switch (stage) {
-        case 0: launch(c, CUMC_K_COMBINE, n, 256, k_combine<COORD, MODEL, 0>, b, c->tabs, pr, ff[0], ff[1], ff[2], a); break;
-        case 1: launch(c, CUMC_K_COMBINE, n, 256, k_combine<COORD, MODEL, 1>, b, c->tabs, pr, ff[0], ff[1], ff[2], a); break;
-        case 2: launch(c, CUMC_K_COMBINE, n, 256, k_combine<COORD, MODEL, 2>, b, c->tabs, pr, ff[0], ff[1], ff[2], a); break;
-        default: launch(c, CUMC_K_COMBINE, n, 256, k_combine<COORD, MODEL, 3>, b, c->tabs, pr, ff[0], ff[1], ff[2], a); break;
-    }
-}
-
-template <int COORD>
-void combine_model(cumc_ctx* c, const Box& b, int stage, const Prim& pr, const FaceFlux* ff, const CombineArgs& a) {
-    switch (c->model) {
-        case CUMC_MODEL_NONE: combine_dispatch<COORD, 0>(c, b, stage, pr, ff, a); break;
-        case CUMC_MODEL_RIEMANN: combine_dispatch<COORD, 1>(c, b, stage, pr, ff, a); break;
-        case CUMC_MODEL_TORUS_SPH: combine_dispatch<COORD, 2>(c, b, stage, pr, ff, a); break;
-        default: combine_dispatch<COORD, 3>(c, b, stage, pr, ff, a); break;
-    }
-}
-
 // primitive buffers of one state: the context's own, or an adjoint scratch set
 struct PrimBufs {
     double* const* w;
@@ -294,7 +273,45 @@ struct PrimBufs {
     double* eps;
 };
 
-void utop_into(cumc_ctx* c, const Box& b, double* const* u, const PrimBufs& p, bool from_cons) {
+UtopArgs utop_args(cumc_ctx* c, double* const* u, const PrimBufs& p);
+
+// stage 0: l_rk alone; stages 1-3: face fields, then hydro combine + conversions
+template <int COORD, int MODEL, int STAGE>
+void combine_stage(cumc_ctx* c, const Box& b, const Prim& pr, const FaceFlux* ff, const CombineArgs& a,
+                   const UtopArgs& o) {
+    const long long n = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
+    if (STAGE == 0) {
+        launch(c, CUMC_K_COMBINE, n, 256, k_combine<COORD, MODEL>, b, c->tabs, pr, ff[0], ff[1], ff[2], a);
+        return;
+    }
+    constexpr int S = STAGE == 0 ? 1 : STAGE;
+    launch(c, CUMC_K_CT, n, 256, k_ct<COORD, S>, b, c->tabs, a);
+    launch(c, CUMC_K_COMBINE, n, 256, k_combine_utop<COORD, MODEL, S>, b, c->tabs, pr, ff[0], ff[1], ff[2], a, o);
+}
+
+template <int COORD, int MODEL>
+void combine_dispatch(cumc_ctx* c, const Box& b, int stage, const Prim& pr, const FaceFlux* ff, const CombineArgs& a,
+                      const UtopArgs& o) {
+    switch (stage) {
+        case 0: combine_stage<COORD, MODEL, 0>(c, b, pr, ff, a, o); break;
+        case 1: combine_stage<COORD, MODEL, 1>(c, b, pr, ff, a, o); break;
+        case 2: combine_stage<COORD, MODEL, 2>(c, b, pr, ff, a, o); break;
+        default: combine_stage<COORD, MODEL, 3>(c, b, pr, ff, a, o); break;
+    }
+}
+
+template <int COORD>
+void combine_model(cumc_ctx* c, const Box& b, int stage, const Prim& pr, const FaceFlux* ff, const CombineArgs& a,
+                   const UtopArgs& o) {
+    switch (c->model) {
+        case CUMC_MODEL_NONE: combine_dispatch<COORD, 0>(c, b, stage, pr, ff, a, o); break;
+        case CUMC_MODEL_RIEMANN: combine_dispatch<COORD, 1>(c, b, stage, pr, ff, a, o); break;
+        case CUMC_MODEL_TORUS_SPH: combine_dispatch<COORD, 2>(c, b, stage, pr, ff, a, o); break;
+        default: combine_dispatch<COORD, 3>(c, b, stage, pr, ff, a, o); break;
+    }
+}
+
+UtopArgs utop_args(cumc_ctx* c, double* const* u, const PrimBufs& p) {
     UtopArgs a;
     for (int q = 0; q < 8; ++q) a.u[q] = u[q];
     for (int q = 0; q < 5; ++q) a.w[q] = p.w[q];
@@ -304,6 +321,11 @@ void utop_into(cumc_ctx* c, const Box& b, double* const* u, const PrimBufs& p, b
     a.rho_floor = c->cfg.rho_floor;
     a.eps_floor = c->cfg.eps_floor;
     a.flag = c->flag_dev;
+    return a;
+}
+
+void utop_into(cumc_ctx* c, const Box& b, double* const* u, const PrimBufs& p, bool from_cons) {
+    const UtopArgs a = utop_args(c, u, p);
     const long long n = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
 #define CUMC_UTOP(M)                                                                         \
     if (from_cons) launch(c, CUMC_K_UTOP, n, 256, k_utop<M, true>, b, a);                    \
@@ -408,18 +430,17 @@ void run_stage(cumc_ctx* c, const Box& b, int stage) {
     a.geom_repeat = c->cfg.geom_source_repeat;
     a.rho_floor = c->cfg.rho_floor;
     a.r_sh = c->cfg.r_sh;
+    // adjoint recomputation: the combine's output of this stage, on (0:n)^3.
+    // Nothing reads the hydro cons outside (0:n)^3, nor a face field outside
+    // 0:n along its own axis, and the boundary refills the tangential ones.
+    for (int q = 0; q < 8; ++q) a.tape[q] = (c->tape && stage > 0) ? c->tape[(stage - 1) * 8 + q] : nullptr;
+    const UtopArgs o = utop_args(c, dst, PrimBufs{c->w, c->bc, c->eps});
     switch (c->coord) {
-        case CUMC_CARTESIAN: combine_model<1>(c, b, stage, pr, ff, a); break;
-        case CUMC_CYLINDRICAL: combine_model<2>(c, b, stage, pr, ff, a); break;
-        default: combine_model<3>(c, b, stage, pr, ff, a); break;
+        case CUMC_CARTESIAN: combine_model<1>(c, b, stage, pr, ff, a, o); break;
+        case CUMC_CYLINDRICAL: combine_model<2>(c, b, stage, pr, ff, a, o); break;
+        default: combine_model<3>(c, b, stage, pr, ff, a, o); break;
     }
     if (stage == 0) return;
-    if (c->tape) {  // adjoint recomputation: keep the combine's output of this stage
-        const size_t bytes = (size_t)b.count() * sizeof(double);
-        for (int q = 0; q < 8; ++q)
-            cudaMemcpyAsync(c->tape[(stage - 1) * 8 + q], dst[q], bytes, cudaMemcpyDeviceToDevice, c->stream);
-    }
-    utop(c, b, dst, true);
     boundary(c, b, dst);
 }
 

@@ -3,9 +3,12 @@
 // One SSP-RK3 stage (solver/rungekutta.f90:38-66) runs as
 //   k_sweep<x>, k_sweep<y>, k_sweep<z>   face fluxes (GET_FLUXES interpolate + RIEMANN)
 //   k_emf                                edge EMFs (GET_FLUXES EMF sums + flux_ct ecell/ecorn)
-//   k_combine                            flux difference + sources + CT curl + RK combine
-//   k_utop                               FROMUTORVE, CUSTOM_CHECKRHO, FROMRVETOU, UPDATE (interior)
+//   k_ct                                 CT curl + RK combine of the face fields
+//   k_combine_utop                       flux difference + sources + RK combine of the hydro
+//                                        cons, then FROMUTORVE, CUSTOM_CHECKRHO, FROMRVETOU,
+//                                        UPDATE (interior)
 //   k_boundary                           BOUNDARY (+CUSTOM_BOUNDARY) and UPDATE on the ghosts
+// (k_combine stores l_rk for SPATIAL alone; k_utop serves initial_update.)
 // The reference's intermediates primL/primR/consL/consR/fluxL/fluxR/l_rk/sc/
 // ecell never reach HBM here; only the face fluxes and edge EMFs do.
 #pragma once
@@ -153,40 +156,41 @@ __global__ void __launch_bounds__(256) k_emf(Box b, PrimT<R> pr, FaceFluxT<R> fx
 }
 
 // ----------------------------------------------------------------------------
-// k_combine: l_rk and the RK stage combine on (0:n)^3 (solver/rungekutta.f90
-// :41-51,75-85,109-119). Hydro l_rk (interior only) is the x, y, z flux
-// differences in that order plus the source (solver/spatial.f90:171-187,
-// 365-375); the field l_rk is the CT curl (solver/mhd.f90:130-153).
-// STAGE 0 stores l_rk instead of combining (SPATIAL alone).
+// The RK stage combine on (0:n)^3 (solver/rungekutta.f90:41-51,75-85,109-119).
+// Hydro l_rk (interior only) is the x, y, z flux differences in that order
+// plus the source (solver/spatial.f90:171-187,365-375); the field l_rk is the
+// CT curl (solver/mhd.f90:130-153).
+//
+// Stages 1-3 run as two kernels. k_ct updates the face fields. k_combine_utop
+// then combines the hydro cons in registers and converts them at once
+// (FROMUTORVE, CUSTOM_CHECKRHO, P_to_U, UPDATE's pressure): the cell-centred
+// field it needs averages face fields at i, i-1, i-SX and i-SX*SY, which k_ct
+// has all written by then. The combined hydro cons therefore never make a
+// round trip through HBM between the combine and the conversion. Every value
+// is computed by the same expressions, in the same order, as the combine and
+// k_utop would in sequence. k_combine (STAGE 0 only) stores l_rk for
+// cumc_spatial.
 // ----------------------------------------------------------------------------
 struct CombineArgs {
     const double* u0[8];  // u_old
     const double* uc[8];  // cons entering the combine (stages 2 and 3)
     double* ud[8];        // result (may alias u0 or uc: pointwise)
     double* lrk[8];       // STAGE 0 output
+    double* tape[8];      // when set: a copy of the combine's output, before the conversion
     const double* dt;     // device scalar
     const double* ecorn[3];
     int geom_repeat;
     double rho_floor, r_sh;
 };
 
-template <int COORD, int MODEL, int STAGE>
-__global__ void __launch_bounds__(256) k_combine(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy, FaceFlux fz,
-                                                 CombineArgs a) {
-    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
-    const long long total = (long long)n0 * n1 * n2;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total || (b.skip && *b.skip)) return;
-    const int j = (int)(t % n0);
-    const int k = (int)((t / n0) % n1);
-    const int l = (int)(t / ((long long)n0 * n1));
-    const int i = b.idx(j, k, l);
-    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
-
-    double L[8];
+// hydro l_rk of cell (j, k, l): zero outside the interior
+template <int COORD, int MODEL>
+__device__ __forceinline__ void hydro_lrk(const Tabs& T, const Prim& pr, const FaceFlux& fx, const FaceFlux& fy,
+                                          const FaceFlux& fz, const CombineArgs& a, int j, int k, int l, int i,
+                                          int sk, int sl, double* L) {
+    constexpr int sj = 1;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) L[q] = 0.0;
-
+    for (int q = 0; q < 5; ++q) L[q] = 0.0;
     if (j >= 1 && k >= 1 && l >= 1) {
         double gp, gc, gm;
         geom_flux<COORD, 0>(T, j, k, l, gp, gc, gm);
@@ -240,38 +244,77 @@ __global__ void __launch_bounds__(256) k_combine(Box b, Tabs T, Prim pr, FaceFlu
 #pragma unroll
         for (int q = 0; q < 5; ++q) L[q] = L[q] + sc[q];
     }
+}
 
-    // CT update of the face fields (solver/mhd.f90:137-148)
-    {
-        CTf g;
-        geom_ct<COORD>(T, j, k, l, g);
-        const double* Ex = a.ecorn[0];
-        const double* Ey = a.ecorn[1];
-        const double* Ez = a.ecorn[2];
-        L[IBX] = -((Ez[i] * g.bx_ez_p - Ez[i - sk] * g.bx_ez_m) / g.bx_ez_c -
-                   (Ey[i] * g.bx_ey_p - Ey[i - sl] * g.bx_ey_m) / g.bx_ey_c);
-        L[IBY] = -((Ex[i] * g.by_ex_p - Ex[i - sl] * g.by_ex_m) / g.by_ex_c -
-                   (Ez[i] * g.by_ez_p - Ez[i - sj] * g.by_ez_m) / g.by_ez_c);
-        L[IBZ] = -((Ey[i] * g.bz_ey_p - Ey[i - sj] * g.bz_ey_m) / g.bz_ey_c -
-                   (Ex[i] * g.bz_ex_p - Ex[i - sk] * g.bz_ex_m) / g.bz_ex_c);
-    }
+// field l_rk of face triple (j, k, l): the CT update (solver/mhd.f90:137-148)
+template <int COORD>
+__device__ __forceinline__ void ct_lrk(const Tabs& T, const double* const* ecorn, int j, int k, int l, int i, int sk,
+                                       int sl, double* L) {
+    constexpr int sj = 1;
+    CTf g;
+    geom_ct<COORD>(T, j, k, l, g);
+    const double* Ex = ecorn[0];
+    const double* Ey = ecorn[1];
+    const double* Ez = ecorn[2];
+    L[0] = -((Ez[i] * g.bx_ez_p - Ez[i - sk] * g.bx_ez_m) / g.bx_ez_c -
+             (Ey[i] * g.bx_ey_p - Ey[i - sl] * g.bx_ey_m) / g.bx_ey_c);
+    L[1] = -((Ex[i] * g.by_ex_p - Ex[i - sl] * g.by_ex_m) / g.by_ex_c -
+             (Ez[i] * g.by_ez_p - Ez[i - sj] * g.by_ez_m) / g.by_ez_c);
+    L[2] = -((Ey[i] * g.bz_ey_p - Ey[i - sj] * g.bz_ey_m) / g.bz_ey_c -
+             (Ex[i] * g.bz_ex_p - Ex[i - sk] * g.bz_ex_m) / g.bz_ex_c);
+}
 
-    if (STAGE == 0) {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) a.lrk[q][i] = L[q];
-        return;
-    }
-    const double dt = *a.dt;
+// u_new of one value for RK stage STAGE (u_c is not read at stage 1)
+template <int STAGE>
+__device__ __forceinline__ double rk_point(double u0, double uc, double dt, double L) {
     constexpr double rk20 = 3.0 / 4.0, rk21 = 1.0 / 4.0, rk22 = 1.0 / 4.0;
     constexpr double rk30 = 1.0 / 3.0, rk31 = 2.0 / 3.0, rk32 = 2.0 / 3.0;
+    if (STAGE == 1) return u0 + dt * L;
+    if (STAGE == 2) return (rk20 * u0 + rk21 * uc) + (rk22 * dt) * L;
+    return (rk30 * u0 + rk31 * uc) + (rk32 * dt) * L;
+}
+
+// flat thread index -> (j, k, l) on (0:n)^3; false past the end or when skipped
+__device__ __forceinline__ bool box1_index(const Box& b, int& j, int& k, int& l, int& i) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total || (b.skip && *b.skip)) return false;
+    j = (int)(t % n0);
+    k = (int)((t / n0) % n1);
+    l = (int)(t / ((long long)n0 * n1));
+    i = b.idx(j, k, l);
+    return true;
+}
+
+// SPATIAL alone (cumc_spatial): l_rk of all 8 variables
+template <int COORD, int MODEL>
+__global__ void __launch_bounds__(256) k_combine(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy, FaceFlux fz,
+                                                 CombineArgs a) {
+    int j, k, l, i;
+    if (!box1_index(b, j, k, l, i)) return;
+    const int sk = b.SX, sl = b.SX * b.SY;
+    double L[8];
+    hydro_lrk<COORD, MODEL>(T, pr, fx, fy, fz, a, j, k, l, i, sk, sl, L);
+    ct_lrk<COORD>(T, a.ecorn, j, k, l, i, sk, sl, L + IBX);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const double u0 = a.u0[q][i];
-        double r;
-        if (STAGE == 1) r = u0 + dt * L[q];
-        else if (STAGE == 2) r = (rk20 * u0 + rk21 * a.uc[q][i]) + (rk22 * dt) * L[q];
-        else r = (rk30 * u0 + rk31 * a.uc[q][i]) + (rk32 * dt) * L[q];
-        a.ud[q][i] = r;
+    for (int q = 0; q < 8; ++q) a.lrk[q][i] = L[q];
+}
+
+// face fields of RK stage STAGE. Each thread reads u0, uc and writes ud at its
+// own index only, so ud may alias u0 or uc.
+template <int COORD, int STAGE>
+__global__ void __launch_bounds__(256) k_ct(Box b, Tabs T, CombineArgs a) {
+    int j, k, l, i;
+    if (!box1_index(b, j, k, l, i)) return;
+    double L[3];
+    ct_lrk<COORD>(T, a.ecorn, j, k, l, i, b.SX, b.SX * b.SY, L);
+    const double dt = *a.dt;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double r = rk_point<STAGE>(a.u0[IBX + q][i], STAGE == 1 ? 0.0 : a.uc[IBX + q][i], dt, L[q]);
+        a.ud[IBX + q][i] = r;
+        if (a.tape[IBX + q]) a.tape[IBX + q][i] = r;
     }
 }
 
@@ -291,20 +334,11 @@ struct UtopArgs {
     unsigned int* flag;  // bit 0: non-finite value seen
 };
 
-template <int MODEL, bool FROM_CONS>
-__global__ void __launch_bounds__(256) k_utop(Box b, UtopArgs a) {
-    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
-    const long long total = (long long)n0 * n1 * n2;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total || (b.skip && *b.skip)) return;
-    const int j = (int)(t % n0);
-    const int k = (int)((t / n0) % n1);
-    const int l = (int)(t / ((long long)n0 * n1));
-    const int i = b.idx(j, k, l);
-    const bool interior = j >= 1 && k >= 1 && l >= 1;
-
-    double bx, by, bz;
-    if (interior) {  // bcell from the face fields (solver/fromrvetou.f90:97-107, 40-50)
+// bcell of cell i: the face-field average on the interior (solver/fromrvetou.f90
+// :97-107, 40-50, stored), the stored bcell elsewhere
+__device__ __forceinline__ void bcell_point(const Box& b, const UtopArgs& a, int i, bool interior, double& bx,
+                                            double& by, double& bz) {
+    if (interior) {
         bx = 0.5 * (a.u[IBX][i] + a.u[IBX][i - 1]);
         by = 0.5 * (a.u[IBY][i] + a.u[IBY][i - b.SX]);
         bz = 0.5 * (a.u[IBZ][i] + a.u[IBZ][i - b.SX * b.SY]);
@@ -316,15 +350,21 @@ __global__ void __launch_bounds__(256) k_utop(Box b, UtopArgs a) {
         by = a.bc[1][i];
         bz = a.bc[2][i];
     }
+}
+
+// the conversions of one cell; with FROM_CONS the hydro cons come in uh
+template <int MODEL, bool FROM_CONS>
+__device__ __forceinline__ void utop_point(const UtopArgs& a, int i, bool interior, const double* uh, double bx,
+                                           double by, double bz) {
     const double bsquare = (bx * bx + by * by) + bz * bz;
     double rho, vx, vy, vz, e;
     if (FROM_CONS) {
-        rho = a.u[IRHO][i];
-        vx = a.u[IVX][i] / rho;
-        vy = a.u[IVY][i] / rho;
-        vz = a.u[IVZ][i] / rho;
+        rho = uh[IRHO];
+        vx = uh[IVX] / rho;
+        vy = uh[IVY] / rho;
+        vz = uh[IVZ] / rho;
         const double vsquare = (vx * vx + vy * vy) + vz * vz;
-        e = (a.u[ITAU][i] - 0.5 * bsquare) / rho - 0.5 * vsquare;
+        e = (uh[ITAU] - 0.5 * bsquare) / rho - 0.5 * vsquare;
     } else {
         rho = a.w[0][i];
         vx = a.w[1][i];
@@ -356,6 +396,44 @@ __global__ void __launch_bounds__(256) k_utop(Box b, UtopArgs a) {
         a.w[4][i] = p;
         if (!(isfinite(p) && isfinite(vsquare) && isfinite(rho))) atomicOr(a.flag, 1u);
     }
+}
+
+template <int MODEL, bool FROM_CONS>
+__global__ void __launch_bounds__(256) k_utop(Box b, UtopArgs a) {
+    int j, k, l, i;
+    if (!box1_index(b, j, k, l, i)) return;
+    const bool interior = j >= 1 && k >= 1 && l >= 1;
+    double bx, by, bz;
+    bcell_point(b, a, i, interior, bx, by, bz);
+    double uh[5];
+    if (FROM_CONS) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) uh[q] = a.u[q][i];
+    }
+    utop_point<MODEL, FROM_CONS>(a, i, interior, uh, bx, by, bz);
+}
+
+// hydro part of RK stage STAGE and the conversions, after k_ct of the same
+// stage. o.u is a.ud; w, bc and eps of o are the arrays pr reads, each at the
+// thread's own index only, before the thread writes them.
+template <int COORD, int MODEL, int STAGE>
+__global__ void __launch_bounds__(256) k_combine_utop(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy, FaceFlux fz,
+                                                      CombineArgs a, UtopArgs o) {
+    int j, k, l, i;
+    if (!box1_index(b, j, k, l, i)) return;
+    double L[5];
+    hydro_lrk<COORD, MODEL>(T, pr, fx, fy, fz, a, j, k, l, i, b.SX, b.SX * b.SY, L);
+    const double dt = *a.dt;
+    double uh[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        uh[q] = rk_point<STAGE>(a.u0[q][i], STAGE == 1 ? 0.0 : a.uc[q][i], dt, L[q]);
+        if (a.tape[q]) a.tape[q][i] = uh[q];
+    }
+    const bool interior = j >= 1 && k >= 1 && l >= 1;
+    double bx, by, bz;
+    bcell_point(b, o, i, interior, bx, by, bz);
+    utop_point<MODEL, true>(o, i, interior, uh, bx, by, bz);
 }
 
 // ----------------------------------------------------------------------------

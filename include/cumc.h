@@ -164,11 +164,12 @@ int cumc_get_stream(cumc_ctx* ctx, void** stream);
 #define CUMC_K_SWEEP_Y  1
 #define CUMC_K_SWEEP_Z  2
 #define CUMC_K_EMF      3
-#define CUMC_K_COMBINE  4
-#define CUMC_K_UTOP     5
+#define CUMC_K_COMBINE  4   /* FP64 stages: hydro combine fused with the conversions */
+#define CUMC_K_UTOP     5   /* FP64: initial_update's conversions */
 #define CUMC_K_BOUNDARY 6
 #define CUMC_K_FINDDT   7
-#define CUMC_K_COUNT    8
+#define CUMC_K_CT       8   /* FP64 stages: face-field (CT) combine */
+#define CUMC_K_COUNT    9
 int cumc_profile(cumc_ctx* ctx, int enable);
 int cumc_profile_read(cumc_ctx* ctx, int which, int* launches, double* ms);
 
