@@ -382,11 +382,14 @@ namespace cumc {
 // fluxes are bit-identical); lanes 2..28 then solve HLL at their faces. A
 // warp yields 27 faces; consecutive warps overlap by 5 cells. Loads and
 // stores are one 256-byte row segment per field.
+// Eight 128-thread blocks per SM (64 registers, a few spilled to L1): the
+// kernel is bound by FP64 dependency latency, and 32 resident warps hide more
+// of it than 20 unspilled ones (1.46 -> 1.25 ms at 256^3).
 // ---------------------------------------------------------------------------
 constexpr int XW_FACES = 27;
 
 template <int RECON, typename R>
-__global__ void __launch_bounds__(128) k_sweep_xwarp(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out) {
+__global__ void __launch_bounds__(128, 8) k_sweep_xwarp(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out) {
     constexpr unsigned FULL = 0xffffffffu;
     const int nw = (b.nx + 1 + XW_FACES - 1) / XW_FACES;  // warps per row
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
