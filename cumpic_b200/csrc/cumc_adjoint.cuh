@@ -449,9 +449,10 @@ struct FaceAdj {
 // sweep^T, pass A: per face (normal 0:n_d, transverse 0:n+1), the flux
 // adjoints from mu (flux difference) and the edge adjoints (emf), the forward
 // left/right states, and HLL^T. Writes the state adjoints to fa and adds the
-// normal-field adjoint of the face to lambf.
+// normal-field adjoint of the face to lambf. Five 128-thread blocks per SM:
+// 96 registers with some spilled to L1 beat 166 registers at three blocks.
 template <int DIR, int RECON>
-__global__ void __launch_bounds__(128) k_adj_hll(Box b, Tabs T, Prim pr, double ggas, AdjStage a, FaceAdj fa,
+__global__ void __launch_bounds__(128, 5) k_adj_hll(Box b, Tabs T, Prim pr, double ggas, AdjStage a, FaceAdj fa,
                                                 double* lambf) {
     const int n0 = (DIR == 0 ? b.nx : b.nx + 1) + 1;
     const int n1 = (DIR == 1 ? b.ny : b.ny + 1) + 1;
@@ -662,13 +663,116 @@ __global__ void __launch_bounds__(128) k_adj_recon_x(Box b, Tabs T, Prim pr, Fac
     }
 }
 
-// boundary^T: the transpose of k_boundary. Each ghost's adjoint (after the
-// ghost-pressure term p = rho eps (gamma-1), solver/update.f90:27-35) is added,
-// with the parity sign, to the active cell (or live face) it was copied from,
-// then cleared. Several ghosts share a source (corners, outflow copies), so
-// the additions are atomic. fw holds the forward primitives of the stage.
-__global__ void __launch_bounds__(256) k_adj_boundary(Box b, BoundArgs fw, AdjPrim o, double* lbx, double* lby,
-                                                      double* lbz) {
+// boundary^T: the transpose of k_boundary, in gather form. k_boundary copies
+// each ghost from one source (an active cell, or a live face), with the
+// parity sign, and sets the ghost pressure p = rho eps (gamma-1)
+// (solver/update.f90:27-35). So the transpose adds to each source the signed
+// adjoints of every ghost copied from it, each ghost's density and eps
+// adjoints first taking in its pressure adjoint. k_adj_boundary_gather runs
+// one thread per possible source and enumerates its ghost images direction
+// by direction (at most 6 per direction), so there are no atomics and the
+// summation order is fixed. k_adj_boundary_clear then zeroes every ghost
+// adjoint that was moved. fw holds the forward primitives of the stage.
+
+// ghost indices along one direction whose gmap source is a; count returned
+__device__ __forceinline__ int ghost_images(int a, int n, int fin, int fout, int* g, int* side) {
+    int c = 0;
+    if (a < 1 || a > n) return 0;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+        const int i = t < 3 ? t - 2 : n + t - 2;
+        int src, sd;
+        gmap(i, n, fin, fout, src, sd);
+        if (src == a) {
+            g[c] = i;
+            side[c] = sd;
+            ++c;
+        }
+    }
+    return c;
+}
+
+// parity factor of a ghost image (side < 0: identity)
+__device__ __forceinline__ int bsign(const BoundArgs& fw, int dir, int side, int q) {
+    if (side < 0 || fw.flag[2 * dir + side] < 2) return 1;
+    return fw.fac[2 * dir + side][q];
+}
+
+__global__ void __launch_bounds__(256) k_adj_boundary_gather(Box b, BoundArgs fw, AdjPrim o, double* lbx, double* lby,
+                                                             double* lbz) {
+    int j, k, l, i;
+    if (!box1_index(b, j, k, l, i)) return;
+    // index lists per direction: entry 0 is the identity, then the ghost images
+    int gx[7], sx[7], gy[7], sy[7], gz[7], sz[7], gye[7], sye[7];
+    gx[0] = j, gy[0] = k, gz[0] = l, gye[0] = k;
+    sx[0] = sy[0] = sz[0] = sye[0] = -1;
+    const int cx = 1 + ghost_images(j, b.nx, fw.flag[0], fw.flag[1], gx + 1, sx + 1);
+    const int cy = 1 + ghost_images(k, b.ny, fw.flag[2], fw.flag[3], gy + 1, sy + 1);
+    const int cz = 1 + ghost_images(l, b.nz, fw.flag[4], fw.flag[5], gz + 1, sz + 1);
+    const int cye = 1 + ghost_images(k, b.ny, fw.flag[2], fw.eps_yout, gye + 1, sye + 1);
+    if (cx == 1 && cy == 1 && cz == 1 && cye == 1) return;
+    const double gm1 = fw.ggas - 1.0;
+    if (j >= 1 && k >= 1 && l >= 1) {  // cell-centred quantities
+        double acc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int z = 0; z < cz; ++z)
+            for (int y = 0; y < cy; ++y)
+                for (int x = 0; x < cx; ++x) {
+                    if (x == 0 && y == 0 && z == 0) continue;
+                    const int g = b.idx(gx[x], gy[y], gz[z]);
+                    const double lp = o.w[4][g];
+                    const double lw[7] = {o.w[0][g] + lp * fw.eps[g] * gm1, o.w[1][g], o.w[2][g], o.w[3][g],
+                                          o.bc[0][g], o.bc[1][g], o.bc[2][g]};
+#pragma unroll
+                    for (int q = 0; q < 7; ++q) {
+                        const int qq = q < 4 ? q : IBX + q - 4;
+                        const int s = bsign(fw, 0, sx[x], qq) * bsign(fw, 1, sy[y], qq) * bsign(fw, 2, sz[z], qq);
+                        acc[q] += s * lw[q];
+                    }
+                }
+        double acce = 0.0;
+        for (int z = 0; z < cz; ++z)
+            for (int y = 0; y < cye; ++y)
+                for (int x = 0; x < cx; ++x) {
+                    if (x == 0 && y == 0 && z == 0) continue;
+                    const int g = b.idx(gx[x], gye[y], gz[z]);
+                    acce += o.eps[g] + o.w[4][g] * fw.w[0][g] * gm1;
+                }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (acc[q] != 0.0) o.w[q][i] += acc[q];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            if (acc[4 + q] != 0.0) o.bc[q][i] += acc[4 + q];
+        if (acce != 0.0) o.eps[i] += acce;
+    }
+    // face fields: only the components tangential to a ghost direction move
+    if (k >= 1 && l >= 1 && (cy > 1 || cz > 1)) {
+        double acc = 0.0;
+        for (int z = 0; z < cz; ++z)
+            for (int y = 0; y < cy; ++y)
+                if (y || z) acc += (bsign(fw, 1, sy[y], IBX) * bsign(fw, 2, sz[z], IBX)) * lbx[b.idx(j, gy[y], gz[z])];
+        if (acc != 0.0) lbx[i] += acc;
+    }
+    if (j >= 1 && l >= 1 && (cx > 1 || cz > 1)) {
+        double acc = 0.0;
+        for (int z = 0; z < cz; ++z)
+            for (int x = 0; x < cx; ++x)
+                if (x || z) acc += (bsign(fw, 0, sx[x], IBY) * bsign(fw, 2, sz[z], IBY)) * lby[b.idx(gx[x], k, gz[z])];
+        if (acc != 0.0) lby[i] += acc;
+    }
+    if (j >= 1 && k >= 1 && (cx > 1 || cy > 1)) {
+        double acc = 0.0;
+        for (int y = 0; y < cy; ++y)
+            for (int x = 0; x < cx; ++x)
+                if (x || y) acc += (bsign(fw, 0, sx[x], IBZ) * bsign(fw, 1, sy[y], IBZ)) * lbz[b.idx(gx[x], gy[y], l)];
+        if (acc != 0.0) lbz[i] += acc;
+    }
+}
+
+// zero the ghost adjoints k_adj_boundary_gather moved (one thread per ghost,
+// the ghost order of k_boundary)
+__global__ void __launch_bounds__(256) k_adj_boundary_clear(Box b, BoundArgs fw, AdjPrim o, double* lbx, double* lby,
+                                                            double* lbz) {
     const long long zsl = 6LL * b.SX * b.SY, ysl = 6LL * b.SX * b.nz, xsl = 6LL * b.ny * b.nz;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int j, k, l;
@@ -694,67 +798,15 @@ __global__ void __launch_bounds__(256) k_adj_boundary(Box b, BoundArgs fw, AdjPr
         return;
     }
     const int i = b.idx(j, k, l);
-    int sj, sk, sl, dj, dk, dl;
-    const bool gx = gmap(j, b.nx, fw.flag[0], fw.flag[1], sj, dj);
-    const bool gy = gmap(k, b.ny, fw.flag[2], fw.flag[3], sk, dk);
-    const bool gz = gmap(l, b.nz, fw.flag[4], fw.flag[5], sl, dl);
-    auto sgn = [&](int q) -> double {
-        int s = 1;
-        if (gx && fw.flag[dj] >= 2) s *= fw.fac[dj][q];
-        if (gy && fw.flag[2 + dk] >= 2) s *= fw.fac[2 + dk][q];
-        if (gz && fw.flag[4 + dl] >= 2) s *= fw.fac[4 + dl][q];
-        return (double)s;
-    };
-    const int src = b.idx(sj, sk, sl);
-    // ghost pressure
-    const double lp = o.w[4][i];
-    o.w[4][i] = 0.0;
-    double lrho = o.w[0][i] + lp * fw.eps[i] * (fw.ggas - 1.0);
-    double leps = o.eps[i] + lp * fw.w[0][i] * (fw.ggas - 1.0);
-    const double lw[4] = {lrho, o.w[1][i], o.w[2][i], o.w[3][i]};
+    const bool gx = j < 1 || j > b.nx, gy = k < 1 || k > b.ny, gz = l < 1 || l > b.nz;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        o.w[q][i] = 0.0;
-        if (lw[q] != 0.0) atomicAdd(o.w[q] + src, sgn(q) * lw[q]);
-    }
+    for (int q = 0; q < 5; ++q) o.w[q][i] = 0.0;
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        const double v = o.bc[q][i];
-        o.bc[q][i] = 0.0;
-        if (v != 0.0) atomicAdd(o.bc[q] + src, sgn(IBX + q) * v);
-    }
-    {
-        int ej = j, ek = k, el = l, dd;
-        gmap(j, b.nx, fw.flag[0], fw.flag[1], ej, dd);
-        gmap(k, b.ny, fw.flag[2], fw.eps_yout, ek, dd);
-        gmap(l, b.nz, fw.flag[4], fw.flag[5], el, dd);
-        o.eps[i] = 0.0;
-        if (leps != 0.0) atomicAdd(o.eps + b.idx(ej, ek, el), leps);
-    }
-    if (j >= 0 && j <= b.nx && (gy || gz)) {
-        int s = 1;
-        if (gy && fw.flag[2 + dk] >= 2) s *= fw.fac[2 + dk][IBX];
-        if (gz && fw.flag[4 + dl] >= 2) s *= fw.fac[4 + dl][IBX];
-        const double v = lbx[i];
-        lbx[i] = 0.0;
-        if (v != 0.0) atomicAdd(lbx + b.idx(j, sk, sl), s * v);
-    }
-    if (k >= 0 && k <= b.ny && (gx || gz)) {
-        int s = 1;
-        if (gx && fw.flag[dj] >= 2) s *= fw.fac[dj][IBY];
-        if (gz && fw.flag[4 + dl] >= 2) s *= fw.fac[4 + dl][IBY];
-        const double v = lby[i];
-        lby[i] = 0.0;
-        if (v != 0.0) atomicAdd(lby + b.idx(sj, k, sl), s * v);
-    }
-    if (l >= 0 && l <= b.nz && (gx || gy)) {
-        int s = 1;
-        if (gx && fw.flag[dj] >= 2) s *= fw.fac[dj][IBZ];
-        if (gy && fw.flag[2 + dk] >= 2) s *= fw.fac[2 + dk][IBZ];
-        const double v = lbz[i];
-        lbz[i] = 0.0;
-        if (v != 0.0) atomicAdd(lbz + b.idx(sj, sk, l), s * v);
-    }
+    for (int q = 0; q < 3; ++q) o.bc[q][i] = 0.0;
+    o.eps[i] = 0.0;
+    if (j >= 0 && j <= b.nx && (gy || gz)) lbx[i] = 0.0;
+    if (k >= 0 && k <= b.ny && (gx || gz)) lby[i] = 0.0;
+    if (l >= 0 && l <= b.nz && (gx || gy)) lbz[i] = 0.0;
 }
 
 // utop^T on the active cells: from the adjoints of the re-derived conserved

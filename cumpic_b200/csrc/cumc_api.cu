@@ -1125,6 +1125,13 @@ void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, c
                 0, k_adj_recon_col<2, RECON>, b, c->tabs, pr, fa, lp);
 }
 
+// boundary^T: gather onto the sources, then clear the ghosts
+void adj_boundary(cumc_ctx* c, const Box& b, const BoundArgs& fw, const AdjPrim& lp, double* const* lbf) {
+    launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_boundary_gather, b, fw, lp, lbf[0],
+           lbf[1], lbf[2]);
+    launch(c, -1, ghost_count(b), 256, k_adj_boundary_clear, b, fw, lp, lbf[0], lbf[1], lbf[2]);
+}
+
 template <bool FROM_CONS>
 void adj_utop(cumc_ctx* c, const Box& b, Arr8 u, Arr8 w0, const double* eps0, Arr8 lu, const AdjPrim& lp, Arr8 mu,
               Arr3 lb, double alpha = 0.0, double beta = 0.0, Arr8 lam0 = Arr8{}) {
@@ -1283,8 +1290,7 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
                 else if (n > a0) adj_prims_from(c, b, &tape[(size_t)(n - 1 - a0) * 24 + 16], Pp);
                 else copy_state(c, Pp, ck[seg]);
                 // boundary^T and utop^T of the stage's output
-                launch(c, -1, ghost_count(b), 256, k_adj_boundary, b, bound_args(c, Pc.u, Pc.prim()), lp,
-                       lamCur[IBX], lamCur[IBY], lamCur[IBZ]);
+                adj_boundary(c, b, bound_args(c, Pc.u, Pc.prim()), lp, lamCur + IBX);
                 // utop^T and the face-field gather, each with the combine^T of its part
                 adj_utop<true>(c, b, arr8(tp + (s - 1) * 8), arr8(Pc.w, 5), nullptr, arr8(lamCur), lp, arr8(mu), arr3(lb),
                                alpha[s], beta[s], arr8(lamU0));
@@ -1312,8 +1318,7 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
         }
     }
     // ---- initial_update^T: P[pc] and ck[0] hold the state after initial_update
-    launch(c, -1, ghost_count(b), 256, k_adj_boundary, b, bound_args(c, ck[0].u, ck[0].prim()), lp, lamCur[IBX],
-           lamCur[IBY], lamCur[IBZ]);
+    adj_boundary(c, b, bound_args(c, ck[0].u, ck[0].prim()), lp, lamCur + IBX);
     adj_utop<false>(c, b, arr8(ck[0].u), arr8(ck[0].w, 5), ck[0].eps, arr8(lamCur), lp, arr8(mu), arr3(lb));
     launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_bface, b, arr3(lamCur + IBX), arr3(lb),
            arr3(mu + IBX), 0.0, 0.0, Arr3{});
