@@ -451,7 +451,11 @@ struct FaceAdj {
 // left/right states, and HLL^T. Writes the state adjoints to fa and adds the
 // normal-field adjoint of the face to lambf. Five 128-thread blocks per SM:
 // 96 registers with some spilled to L1 beat 166 registers at three blocks.
-template <int DIR, int RECON>
+// FROM_STATES: fa already holds the forward states (the forward sweep's
+// STATES form, one reconstruction per cell); each face reads its two states
+// and overwrites them with their adjoints. Otherwise the face reconstructs
+// its two cells itself.
+template <int DIR, int RECON, bool FROM_STATES = false>
 __global__ void __launch_bounds__(128, 5) k_adj_hll(Box b, Tabs T, Prim pr, double ggas, AdjStage a, FaceAdj fa,
                                                 double* lambf) {
     const int n0 = (DIR == 0 ? b.nx : b.nx + 1) + 1;
@@ -514,6 +518,11 @@ __global__ void __launch_bounds__(128, 5) k_adj_hll(Box b, Tabs T, Prim pr, doub
     double wl[8], wr[8];
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
+        if (FROM_STATES) {
+            wl[slot[v]] = fa.l[v][base];
+            wr[slot[v]] = fa.r[v][base];
+            continue;
+        }
         const double* q = src[v] + base;
         double cv[6];
 #pragma unroll

@@ -12,6 +12,7 @@
 #include "cumc_adjoint.cuh"
 
 #include <cmath>
+#include <type_traits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -220,9 +221,9 @@ void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
         if (c->sweep_mode == 4 || c->sweep_mode == 0 || c->sweep_mode == 7) {
             const size_t sm = walk_smem<double>(DIR);
             if (c->recon == CUMC_PPMC)
-                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 4, double>, b, c->tabs, pr, c->ggas, out, seg);
+                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 4, double>, b, c->tabs, pr, c->ggas, out, seg, out);
             else
-                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 1, double>, b, c->tabs, pr, c->ggas, out, seg);
+                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 1, double>, b, c->tabs, pr, c->ggas, out, seg, out);
         } else {
             const size_t sm = DIR == 0 ? xstage_smem<double>() : 0;
             if (c->recon == CUMC_PPMC)
@@ -234,9 +235,9 @@ void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
     }
     if (DIR == 0 && (c->sweep_mode == 0 || c->sweep_mode == 6)) {  // x: one lane per cell
         if (c->recon == CUMC_PPMC)
-            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b), 128, k_sweep_xwarp<4, double>, b, c->tabs, pr, c->ggas, out);
+            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b), 128, k_sweep_xwarp<4, double>, b, c->tabs, pr, c->ggas, out, out);
         else
-            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b), 128, k_sweep_xwarp<1, double>, b, c->tabs, pr, c->ggas, out);
+            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b), 128, k_sweep_xwarp<1, double>, b, c->tabs, pr, c->ggas, out, out);
         return;
     }
     if (c->sweep_mode != 2) {  // one thread per face
@@ -1112,15 +1113,32 @@ void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, c
     const long long fx = (long long)(b.nx + 1) * (b.ny + 2) * (b.nz + 2);
     const long long fy = (long long)(b.nx + 2) * (b.ny + 1) * (b.nz + 2);
     const long long fz = (long long)(b.nx + 2) * (b.ny + 2) * (b.nz + 1);
+    // face states of each direction from the forward sweep's STATES form
+    FaceFlux sl, sr;
+    for (int v = 0; v < 7; ++v) {
+        sl.f[v] = fa.l[v];
+        sr.f[v] = fa.r[v];
+    }
+    auto states = [&](auto dir) {
+        constexpr int D = decltype(dir)::value;
+        int nseg;
+        const int seg = walk_segment(WalkGeom<D>::nd(b) + 1, 64, &nseg);
+        const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
+        launch_grid(c, -1, grid, WK_THREADS, walk_smem<double>(D), k_sweep_walk_sm<D, RECON, double, true>, b, c->tabs,
+                    pr, c->ggas, sl, seg, sr);
+    };
     // x: pass A per face, pass B one lane per cell (28 owned cells a warp)
-    launch(c, -1, fx, 128, k_adj_hll<0, RECON>, b, c->tabs, pr, c->ggas, st, fa, lbf[0]);
+    launch(c, -1, xwarp_threads(b), 128, k_sweep_xwarp<RECON, double, true>, b, c->tabs, pr, c->ggas, sl, sr);
+    launch(c, -1, fx, 128, k_adj_hll<0, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[0]);
     const long long xwarps = (long long)(b.ny + 2) * (b.nz + 2) * ((b.nx + 6 + 27) / 28);
     launch(c, -1, xwarps * 32, 128, k_adj_recon_x<RECON>, b, c->tabs, pr, fa, lp);
     // y, z: pass A per face, pass B one thread per (column, field)
-    launch(c, -1, fy, 128, k_adj_hll<1, RECON>, b, c->tabs, pr, c->ggas, st, fa, lbf[1]);
+    states(std::integral_constant<int, 1>{});
+    launch(c, -1, fy, 128, k_adj_hll<1, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[1]);
     launch_grid(c, -1, dim3((unsigned)((WalkGeom<1>::ncols(b) + 127) / 128), 7, (b.ny + 2 + RC_SEG - 1) / RC_SEG), 128,
                 0, k_adj_recon_col<1, RECON>, b, c->tabs, pr, fa, lp);
-    launch(c, -1, fz, 128, k_adj_hll<2, RECON>, b, c->tabs, pr, c->ggas, st, fa, lbf[2]);
+    states(std::integral_constant<int, 2>{});
+    launch(c, -1, fz, 128, k_adj_hll<2, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[2]);
     launch_grid(c, -1, dim3((unsigned)((WalkGeom<2>::ncols(b) + 127) / 128), 7, (b.nz + 2 + RC_SEG - 1) / RC_SEG), 128,
                 0, k_adj_recon_col<2, RECON>, b, c->tabs, pr, fa, lp);
 }

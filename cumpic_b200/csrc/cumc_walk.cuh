@@ -304,9 +304,13 @@ constexpr size_t walk_smem(int dir) {
     return (size_t)WK_SLOTS * WK_FIELDS * WK_THREADS * sizeof(R) + (dir == 0 ? xstage_smem<R>() : 0);
 }
 
-template <int DIR, int RECON, typename R>
+// STATES (y and z only): instead of solving HLL, store each face's
+// reconstructed states, left in out and right in out_r (field order of the
+// sweep, at the face's left cell), for the adjoint's HLL transpose.
+template <int DIR, int RECON, typename R, bool STATES = false>
 __global__ void __launch_bounds__(WK_THREADS) k_sweep_walk_sm(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
-                                                             int seg) {
+                                                             int seg, FaceFluxT<R> out_r) {
+    static_assert(!STATES || DIR != 0, "face states along y and z");
     extern __shared__ __align__(16) unsigned char wk_raw[];
     R* const sm = reinterpret_cast<R*>(wk_raw) + threadIdx.x;
     auto at = [&](int slot, int v) -> R& { return sm[(slot * WK_FIELDS + v) * WK_THREADS]; };
@@ -364,7 +368,18 @@ __global__ void __launch_bounds__(WK_THREADS) k_sweep_walk_sm(Box b, Tabs T, Pri
 #pragma unroll
             for (int v = 0; v < WK_FIELDS; ++v) nxt[v] = DIR == 0 ? X.get(v, j) : C.src[v][(f + 4) * s];
         }
-        walk_flux<DIR>(C, f, wl, wr, ggas, out, bn, X, j);
+        if (STATES) {
+            if (C.active) {
+                const int o = C.base + f * s;
+#pragma unroll
+                for (int v = 0; v < WK_FIELDS; ++v) {
+                    out.f[v][o] = wl[C.slot[v]];
+                    out_r.f[v][o] = wr[C.slot[v]];
+                }
+            }
+        } else {
+            walk_flux<DIR>(C, f, wl, wr, ggas, out, bn, X, j);
+        }
     }
     if (DIR == 0) walk_last(C, X, out);
 }
@@ -388,8 +403,11 @@ namespace cumc {
 // ---------------------------------------------------------------------------
 constexpr int XW_FACES = 27;
 
-template <int RECON, typename R>
-__global__ void __launch_bounds__(128, 8) k_sweep_xwarp(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out) {
+// STATES: store each face's reconstructed states (left in out, right in
+// out_r, field order of the sweep) instead of solving HLL.
+template <int RECON, typename R, bool STATES = false>
+__global__ void __launch_bounds__(128, 8) k_sweep_xwarp(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
+                                                        FaceFluxT<R> out_r) {
     constexpr unsigned FULL = 0xffffffffu;
     const int nw = (b.nx + 1 + XW_FACES - 1) / XW_FACES;  // warps per row
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -427,6 +445,14 @@ __global__ void __launch_bounds__(128, 8) k_sweep_xwarp(Box b, Tabs T, PrimT<R> 
         wr[slot[v]] = __shfl_down_sync(FULL, vm, 1);  // vm_out of cell c+1
     }
     if (lane < 2 || lane > 28 || c < 0 || c > b.nx) return;
+    if (STATES) {
+#pragma unroll
+        for (int v = 0; v < 7; ++v) {
+            out.f[v][base + c] = wl[slot[v]];
+            out_r.f[v][base + c] = wr[slot[v]];
+        }
+        return;
+    }
     const R bn = pr.bf[0][base + c];
     wl[IBX] = bn;
     wr[IBX] = bn;
