@@ -1,6 +1,6 @@
 // cumc_adjoint.cuh — hand-written discrete adjoint of the FP64 RK3 step
-// (Cartesian, models NONE and RIEMANN, PPM or TVD reconstruction, HLL, CT,
-// every boundary flag).
+// (Cartesian, cylindrical and spherical grids, models NONE and RIEMANN, PPM or
+// TVD reconstruction, HLL, CT, every boundary flag).
 //
 // The forward stage s (solver/rungekutta.f90:38-66 and the kernels of
 // cumc_kernels.cuh) is, per stage,
@@ -379,7 +379,12 @@ __device__ __forceinline__ bool in0n(int j, int k, int l, const Box& b) {
     return j >= 0 && j <= b.nx && k >= 0 && k <= b.ny && l >= 0 && l <= b.nz;
 }
 
-// CT^T: edge-EMF adjoints on (0:n)^3 from the field part of mu (solver/mhd.f90:137-148)
+// CT^T: edge-EMF adjoints on (0:n)^3 from the field part of mu (solver/mhd.f90
+// :137-148, with the GEOM_CT factors of solver/coords.f90:310-415). Each face
+// field's l_rk is (E_a p - E_a' m)/c - (E_b p - E_b' m)/c over the triple's
+// factors, so an edge collects p/c from its own triple and m/c from the
+// triples above it.
+template <int COORD>
 __global__ void __launch_bounds__(256) k_adj_ct(Box b, Tabs T, AdjStage a, double* lex, double* ley, double* lez) {
     const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
     const long long total = (long long)n0 * n1 * n2;
@@ -392,18 +397,28 @@ __global__ void __launch_bounds__(256) k_adj_ct(Box b, Tabs T, AdjStage a, doubl
     const double* mx = a.mu[IBX];
     const double* my = a.mu[IBY];
     const double* mz = a.mu[IBZ];
-    const double dx0 = T.ax[0].d[j], dy0 = T.ax[1].d[k], dz0 = T.ax[2].d[l];
-    const bool jp = j + 1 <= b.nx, kp = k + 1 <= b.ny, lp = l + 1 <= b.nz;
-    const double dx1 = T.ax[0].d[j + 1], dy1 = T.ax[1].d[k + 1], dz1 = T.ax[2].d[l + 1];
-    double ez = -mx[i] / dy0 + my[i] / dx0;
-    if (kp) ez += mx[i + sk] / dy1;
-    if (jp) ez -= my[i + sj] / dx1;
-    double ey = mx[i] / dz0 - mz[i] / dx0;
-    if (lp) ey -= mx[i + sl] / dz1;
-    if (jp) ey += mz[i + sj] / dx1;
-    double ex = -my[i] / dz0 + mz[i] / dy0;
-    if (lp) ex += my[i + sl] / dz1;
-    if (kp) ex -= mz[i + sk] / dy1;
+    // the face triple's own CT factors (the edge is its upper one) ...
+    CTf g;
+    geom_ct<COORD>(T, j, k, l, g);
+    double ez = -(mx[i] * g.bx_ez_p) / g.bx_ez_c + (my[i] * g.by_ez_p) / g.by_ez_c;
+    double ey = (mx[i] * g.bx_ey_p) / g.bx_ey_c - (mz[i] * g.bz_ey_p) / g.bz_ey_c;
+    double ex = -(my[i] * g.by_ex_p) / g.by_ex_c + (mz[i] * g.bz_ex_p) / g.bz_ex_c;
+    // ... and those of the triples above it, where the edge is the lower one
+    if (k + 1 <= b.ny) {
+        geom_ct<COORD>(T, j, k + 1, l, g);
+        ez += (mx[i + sk] * g.bx_ez_m) / g.bx_ez_c;
+        ex -= (mz[i + sk] * g.bz_ex_m) / g.bz_ex_c;
+    }
+    if (j + 1 <= b.nx) {
+        geom_ct<COORD>(T, j + 1, k, l, g);
+        ez -= (my[i + sj] * g.by_ez_m) / g.by_ez_c;
+        ey += (mz[i + sj] * g.bz_ey_m) / g.bz_ey_c;
+    }
+    if (l + 1 <= b.nz) {
+        geom_ct<COORD>(T, j, k, l + 1, g);
+        ey -= (mx[i + sl] * g.bx_ey_m) / g.bx_ey_c;
+        ex += (my[i + sl] * g.by_ex_m) / g.by_ex_c;
+    }
     lex[i] = cdt * ex;
     ley[i] = cdt * ey;
     lez[i] = cdt * ez;
@@ -439,6 +454,58 @@ __global__ void __launch_bounds__(256) k_adj_ecell(Box b, Prim pr, const double*
     o.bc[2][i] += ly * vx - lx * vy;
 }
 
+// GEOM_SOURCE^T (solver/coords.f90:127-161) on the interior cells: the
+// geometric source, added geom_repeat times to l_rk of the cell's momentum
+// (and so to Upre with weight gam dt), differentiated with respect to the
+// stage's primitives (rho, v, p, bcell) at the cell.
+template <int COORD>
+__global__ void __launch_bounds__(256) k_adj_source(Box b, Tabs T, Prim pr, AdjStage a, int repeat, AdjPrim o) {
+    const long long total = (long long)b.nx * b.ny * b.nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int j = (int)(t % b.nx) + 1, k = (int)((t / b.nx) % b.ny) + 1, l = (int)(t / ((long long)b.nx * b.ny)) + 1;
+    const int i = b.idx(j, k, l);
+    const double f = (a.gam * *a.dt) * repeat;
+    const double lx = f * a.mu[IVX][i], ly = f * a.mu[IVY][i], lz = f * a.mu[IVZ][i];
+    const double rho = pr.w[0][i], vx = pr.w[1][i], vy = pr.w[2][i], vz = pr.w[3][i];
+    const double bx = pr.bc[0][i], by = pr.bc[1][i], bz = pr.bc[2][i];
+    const double ix = 1.0 / T.ax[0].c[j];
+    double lrho, lvx, lvy, lvz, lp, lbx, lby, lbz;
+    if (COORD == 2) {
+        // sx = ((p + rho vy^2) + |B|^2/2 - by^2)/R, sy = -(rho vx vy - bx by)/R
+        lrho = (lx * (vy * vy) - ly * (vx * vy)) * ix;
+        lvx = -ly * (rho * vy) * ix;
+        lvy = (lx * (2.0 * rho * vy) - ly * (rho * vx)) * ix;
+        lvz = 0.0;
+        lp = lx * ix;
+        lbx = (lx * bx + ly * by) * ix;
+        lby = (ly * bx - lx * by) * ix;
+        lbz = lx * bz * ix;
+    } else {
+        // sx = ((2p + bx^2) + rho (vy^2 + vz^2))/r
+        // sy = ((p + rho vz^2) + |B|^2/2 - bz^2)/(r tan) - (rho vx vy - bx by)/r
+        // sz = -(rho vx vz - bx bz)/r - (rho vy vz - by bz)/(r tan)
+        const double it = ix / T.tanc[k];
+        lrho = lx * (vy * vy + vz * vz) * ix + ly * ((vz * vz) * it - (vx * vy) * ix) -
+               lz * ((vx * vz) * ix + (vy * vz) * it);
+        lvx = -(ly * vy + lz * vz) * rho * ix;
+        lvy = lx * (2.0 * rho * vy) * ix - ly * (rho * vx) * ix - lz * (rho * vz) * it;
+        lvz = lx * (2.0 * rho * vz) * ix + ly * (2.0 * rho * vz) * it - lz * ((rho * vx) * ix + (rho * vy) * it);
+        lp = 2.0 * lx * ix + ly * it;
+        lbx = 2.0 * lx * bx * ix + ly * (bx * it + by * ix) + lz * bz * ix;
+        lby = ly * (by * it + bx * ix) + lz * bz * it;
+        lbz = -ly * bz * it + lz * (bx * ix + by * it);
+    }
+    o.w[0][i] += lrho;
+    o.w[1][i] += lvx;
+    o.w[2][i] += lvy;
+    o.w[3][i] += lvz;
+    o.w[4][i] += lp;
+    o.bc[0][i] += lbx;
+    o.bc[1][i] += lby;
+    o.bc[2][i] += lbz;
+}
+
 // adjoints of the reconstructed left and right states of each face (the 7
 // reconstructed fields in sweep order), stored at the face's left cell
 struct FaceAdj {
@@ -455,7 +522,7 @@ struct FaceAdj {
 // STATES form, one reconstruction per cell); each face reads its two states
 // and overwrites them with their adjoints. Otherwise the face reconstructs
 // its two cells itself.
-template <int DIR, int RECON, bool FROM_STATES = false>
+template <int COORD, int DIR, int RECON, bool FROM_STATES = false>
 __global__ void __launch_bounds__(128, 5) k_adj_hll(Box b, Tabs T, Prim pr, double ggas, AdjStage a, FaceAdj fa,
                                                 double* lambf) {
     const int n0 = (DIR == 0 ? b.nx : b.nx + 1) + 1;
@@ -480,7 +547,23 @@ __global__ void __launch_bounds__(128, 5) k_adj_hll(Box b, Tabs T, Prim pr, doub
                                   : DIR == 1 ? (j >= 1 && j <= b.nx && l >= 1 && l <= b.nz)
                                              : (j >= 1 && j <= b.nx && k >= 1 && k <= b.ny);
         const bool lin = tin && c >= 1, rin = tin && c + 1 <= nd;
-        const double il = lin ? 1.0 / A.d[c] : 0.0, ir = rin ? 1.0 / A.d[c + 1] : 0.0;
+        // the face enters its left cell's flux difference as -F g+/g_c and
+        // its right cell's as +F g-/g_c (Cartesian: 1/dx of each cell)
+        double il = 0.0, ir = 0.0;
+        if (COORD == 1) {
+            il = lin ? 1.0 / A.d[c] : 0.0;
+            ir = rin ? 1.0 / A.d[c + 1] : 0.0;
+        } else {
+            double gp, gc, gm;
+            if (lin) {
+                geom_flux<COORD, DIR>(T, j, k, l, gp, gc, gm);
+                il = gp / gc;
+            }
+            if (rin) {
+                geom_flux<COORD, DIR>(T, j + (DIR == 0), k + (DIR == 1), l + (DIR == 2), gp, gc, gm);
+                ir = gm / gc;
+            }
+        }
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
             const double ml = lin ? a.mu[q][base] : 0.0, mr = rin ? a.mu[q][base + s] : 0.0;
@@ -959,7 +1042,7 @@ __global__ void __launch_bounds__(256) k_adj_bface(Box b, Arr3 lbf, Arr3 lb, Arr
 // and its adjoint seed. kind 1: magnetic energy 0.5 sum |bcell|^2 dV; kind 2:
 // kinetic energy 0.5 sum rho |v|^2 dV; kind 3: sum of weights . cons over the
 // live entries (weights in lamu on entry).
-__global__ void __launch_bounds__(256) k_adj_objective(Box b, Tabs T, Prim pr, Arr8 u, int kind, AdjPrim o,
+__global__ void __launch_bounds__(256) k_adj_objective(Box b, Tabs T, int coord, Prim pr, Arr8 u, int kind, AdjPrim o,
                                                        Arr8 lamu, double* partial) {
     const long long total = (long long)b.nx * b.ny * b.nz;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -967,7 +1050,10 @@ __global__ void __launch_bounds__(256) k_adj_objective(Box b, Tabs T, Prim pr, A
     if (t < total) {
         const int j = (int)(t % b.nx) + 1, k = (int)((t / b.nx) % b.ny) + 1, l = (int)(t / ((long long)b.nx * b.ny)) + 1;
         const int i = b.idx(j, k, l);
-        const double dv = (T.ax[0].d[j] * T.ax[1].d[k]) * T.ax[2].d[l];
+        // cell volume: dx dy dz; R dR dphi dz; (r^3)/3 d(-cos theta) dphi
+        const double dv = coord == CUMC_CARTESIAN     ? (T.ax[0].d[j] * T.ax[1].d[k]) * T.ax[2].d[l]
+                          : coord == CUMC_CYLINDRICAL ? ((T.ax[0].c[j] * T.ax[0].d[j]) * T.ax[1].d[k]) * T.ax[2].d[l]
+                                                      : (T.r3d3[j] * T.dcos[k]) * T.ax[2].d[l];
         if (kind == 1) {
             const double bx = pr.bc[0][i], by = pr.bc[1][i], bz = pr.bc[2][i];
             acc = 0.5 * ((bx * bx + by * by) + bz * bz) * dv;

@@ -1107,7 +1107,7 @@ Arr3 arr3(double* const* p) {
     return a;
 }
 
-template <int RECON>
+template <int COORD, int RECON>
 void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, const AdjPrim& lp, double* const* lbf,
                 const FaceAdj& fa) {
     const long long fx = (long long)(b.nx + 1) * (b.ny + 2) * (b.nz + 2);
@@ -1129,16 +1129,16 @@ void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, c
     };
     // x: pass A per face, pass B one lane per cell (28 owned cells a warp)
     launch(c, -1, xwarp_threads(b), 128, k_sweep_xwarp<RECON, double, true>, b, c->tabs, pr, c->ggas, sl, sr);
-    launch(c, -1, fx, 128, k_adj_hll<0, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[0]);
+    launch(c, -1, fx, 128, k_adj_hll<COORD, 0, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[0]);
     const long long xwarps = (long long)(b.ny + 2) * (b.nz + 2) * ((b.nx + 6 + 27) / 28);
     launch(c, -1, xwarps * 32, 128, k_adj_recon_x<RECON>, b, c->tabs, pr, fa, lp);
     // y, z: pass A per face, pass B one thread per (column, field)
     states(std::integral_constant<int, 1>{});
-    launch(c, -1, fy, 128, k_adj_hll<1, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[1]);
+    launch(c, -1, fy, 128, k_adj_hll<COORD, 1, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[1]);
     launch_grid(c, -1, dim3((unsigned)((WalkGeom<1>::ncols(b) + 127) / 128), 7, (b.ny + 2 + RC_SEG - 1) / RC_SEG), 128,
                 0, k_adj_recon_col<1, RECON>, b, c->tabs, pr, fa, lp);
     states(std::integral_constant<int, 2>{});
-    launch(c, -1, fz, 128, k_adj_hll<2, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[2]);
+    launch(c, -1, fz, 128, k_adj_hll<COORD, 2, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[2]);
     launch_grid(c, -1, dim3((unsigned)((WalkGeom<2>::ncols(b) + 127) / 128), 7, (b.nz + 2 + RC_SEG - 1) / RC_SEG), 128,
                 0, k_adj_recon_col<2, RECON>, b, c->tabs, pr, fa, lp);
 }
@@ -1148,6 +1148,23 @@ void adj_boundary(cumc_ctx* c, const Box& b, const BoundArgs& fw, const AdjPrim&
     launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_boundary_gather, b, fw, lp, lbf[0],
            lbf[1], lbf[2]);
     launch(c, -1, ghost_count(b), 256, k_adj_boundary_clear, b, fw, lp, lbf[0], lbf[1], lbf[2]);
+}
+
+// SPATIAL^T of one stage: CT^T, ecell^T, GEOM_SOURCE^T (curvilinear grids)
+// and the sweeps' transposes, all adding to the adjoints of the stage's
+// input primitives (lp) and face fields (lbf)
+template <int COORD>
+void adj_spatial(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, const AdjPrim& lp,
+                 double* const* lbf, const FaceAdj& fa, double* const* lamE) {
+    launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_ct<COORD>, b, c->tabs, st, lamE[0],
+           lamE[1], lamE[2]);
+    launch(c, -1, (long long)(b.nx + 2) * (b.ny + 2) * (b.nz + 2), 256, k_adj_ecell, b, pr, (const double*)lamE[0],
+           (const double*)lamE[1], (const double*)lamE[2], lp);
+    if (COORD != 1)
+        launch(c, -1, (long long)b.nx * b.ny * b.nz, 256, k_adj_source<COORD == 1 ? 2 : COORD>, b, c->tabs, pr, st,
+               c->cfg.geom_source_repeat, lp);
+    if (c->recon == CUMC_PPMC) adj_sweeps<COORD, 4>(c, b, pr, st, lp, lbf, fa);
+    else adj_sweeps<COORD, 1>(c, b, pr, st, lp, lbf, fa);
 }
 
 template <bool FROM_CONS>
@@ -1274,7 +1291,7 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
         if ((rc = put_soa(c, weights, 8, lamCur)) != CUMC_OK) return rc;
         launch(c, -1, (long long)NT, 256, k_adj_mask_live, b, arr8(lamCur));
     }
-    launch(c, -1, ncell, 256, k_adj_objective, b, c->tabs, fin.as_prim(), arr8(fin.u), obj, lp, arr8(lamCur), partial);
+    launch(c, -1, ncell, 256, k_adj_objective, b, c->tabs, c->coord, fin.as_prim(), arr8(fin.u), obj, lp, arr8(lamCur), partial);
     launch(c, -1, 256, 256, k_adj_sum, (const double*)partial, nblk, partial + nblk);
     CUMC_CHECK(cudaMemcpyAsync(c->host_pinned, partial + nblk, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CUMC_CHECK(cudaStreamSynchronize(c->stream));
@@ -1321,14 +1338,13 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
                 for (int q = 0; q < 3; ++q) st.lamE[q] = lamE[q];
                 st.dt = ddt + n;
                 st.gam = gam[s];
-                launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_adj_ct, b, c->tabs, st,
-                       lamE[0], lamE[1], lamE[2]);
                 const Prim pr = Pp.as_prim();
-                launch(c, -1, (long long)(b.nx + 2) * (b.ny + 2) * (b.nz + 2), 256, k_adj_ecell, b, pr,
-                       (const double*)lamE[0], (const double*)lamE[1], (const double*)lamE[2], lp);
                 double* const* lbf = s >= 2 ? lamCur + IBX : lamU0 + IBX;
-                if (c->recon == CUMC_PPMC) adj_sweeps<4>(c, b, pr, st, lp, lbf, fa);
-                else adj_sweeps<1>(c, b, pr, st, lp, lbf, fa);
+                switch (c->coord) {
+                    case CUMC_CARTESIAN: adj_spatial<1>(c, b, pr, st, lp, lbf, fa, lamE); break;
+                    case CUMC_CYLINDRICAL: adj_spatial<2>(c, b, pr, st, lp, lbf, fa, lamE); break;
+                    default: adj_spatial<3>(c, b, pr, st, lp, lbf, fa, lamE); break;
+                }
                 pc = 1 - pc;
             }
             std::swap(lamCur, lamU0);  // adjoint of the step's starting state
@@ -1362,9 +1378,8 @@ extern "C" int cumc_adjoint_run(cumc_ctx* c, int nsteps, int checkpoint_every, i
                                 const double* dt_in, double* dt_out, double* J, double* grad_prim, double* grad_eps) {
     if (!c) return CUMC_ERR_ARG;
     if (!c->uploaded) return c->fail(CUMC_ERR_STATE, "cumc_upload_state must come first");
-    if (c->mixed || c->coord != CUMC_CARTESIAN ||
-        (c->model != CUMC_MODEL_NONE && c->model != CUMC_MODEL_RIEMANN))
-        return c->fail(CUMC_ERR_CONFIG, "the adjoint covers CUMC_FP64 on CUMC_CARTESIAN grids with model NONE or RIEMANN");
+    if (c->mixed || (c->model != CUMC_MODEL_NONE && c->model != CUMC_MODEL_RIEMANN))
+        return c->fail(CUMC_ERR_CONFIG, "the adjoint covers CUMC_FP64 with model NONE or RIEMANN");
     if (nsteps < 1 || checkpoint_every < 1) return c->fail(CUMC_ERR_ARG, "nsteps and checkpoint_every must be >= 1");
     if (objective < CUMC_OBJ_MAGNETIC || objective > CUMC_OBJ_LINEAR) return c->fail(CUMC_ERR_ARG, "unknown objective");
     if (objective == CUMC_OBJ_LINEAR && !weights) return c->fail(CUMC_ERR_ARG, "CUMC_OBJ_LINEAR needs weights");

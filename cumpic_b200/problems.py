@@ -231,6 +231,41 @@ def fourier_box(n: int = 128, ggas: float = 5.0 / 3.0, cfl: float = 0.4, modes: 
                    prim, eps, model=N.MODEL_RIEMANN)
 
 
+def shell(coordinate: int, nx: int = 16, ny: int = 12, nz: int = 10, ggas: float = 5.0 / 3.0, cfl: float = 0.4,
+          seed: int = 5, boundary_flag: tuple | None = None, recon: int = N.PPMC) -> Problem:
+    """Smooth magnetised state on a curvilinear grid, for the geometric terms
+    (flux-difference and CT factors, GEOM_SOURCE) without a model's source:
+    a cylindrical annulus R in [1, 2], phi in [0, pi], z in [0, 1], or a
+    spherical shell r in [1, 2], theta in [pi/4, 3pi/4], phi in [0, pi/2].
+    Every field varies smoothly (seeded phases): rho, p = 1 + 0.2 s, v = 0.1 s,
+    B = 0.3 + 0.1 s, with s a sum of sines of the cell's index coordinates.
+    Default flags: copy at both radial ends, mirror at the theta ends, the
+    rest periodic."""
+    if coordinate == N.CYLINDRICAL:
+        xf, yf, zf = uniform_faces(1.0, 2.0, nx), uniform_faces(0.0, math.pi, ny), uniform_faces(0.0, 1.0, nz)
+        flags = (1, 1, 0, 0, 0, 0)
+    elif coordinate == N.SPHERICAL:
+        xf = uniform_faces(1.0, 2.0, nx)
+        yf = uniform_faces(0.25 * math.pi, 0.75 * math.pi, ny)
+        zf = uniform_faces(0.0, 0.5 * math.pi, nz)
+        flags = (1, 1, 2, 2, 0, 0)
+    else:
+        raise ValueError("shell() builds a cylindrical or spherical grid")
+    prim, eps = _empty(nx, ny, nz)
+    X = ((np.arange(-3, nx + 3) + 0.5) / nx)[None, None, :]
+    Y = ((np.arange(-3, ny + 3) + 0.5) / ny)[None, :, None]
+    Z = ((np.arange(-3, nz + 3) + 0.5) / nz)[:, None, None]
+    ph = 2.0 * math.pi * uniform01(seed, np.arange(24, dtype=np.int64)).reshape(8, 3)
+    for q in range(8):
+        s = (np.sin(2 * math.pi * X + ph[q, 0]) * np.cos(2 * math.pi * Y + ph[q, 1]) +
+             np.sin(2 * math.pi * Z + ph[q, 2]))
+        prim[..., q] = (1.0 + 0.2 * s if q in (IRHO, ITAU) else 0.1 * s if q <= IVZ else 0.3 + 0.1 * s)
+    eps[...] = prim[..., ITAU] / prim[..., IRHO] / (ggas - 1.0)
+    return Problem(f"shell_{coordinate}_{nx}x{ny}x{nz}", nx, ny, nz, xf, yf, zf, coordinate,
+                   tuple(boundary_flag) if boundary_flag is not None else flags, ggas, cfl, 0.0, prim, eps,
+                   recon=recon, model=N.MODEL_RIEMANN)
+
+
 def torus(nr: int = 192, nth: int = 128, nph: int = 64, ggas: float = 5.0 / 3.0, cfl: float = 0.4,
           r_in: float = 2.0, r_out: float = 50.0, s_in: float = 6.0, s_max: float = 10.0, q_grad: float = 2.0,
           rho_max: float = 1.0, rho_fac: float = 1.0e-5, rho_cut: float = 0.2, beta: float = 100.0,

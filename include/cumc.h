@@ -205,9 +205,12 @@ int cumc_launch_count(cumc_ctx* ctx, long long* count);
  *            dJ/d(face Bx, By, Bz) in slots 6-8; grad_eps (eps layout, may be
  *            NULL): dJ/d(eps). Ghost entries, which initial_update
  *            overwrites, get 0.
+ * dV is the cell volume: dx dy dz (Cartesian), R dR dphi dz (cylindrical),
+ * (r^3)/3 d(-cos theta) dphi over the cell (spherical).
  * On return the context holds the final state, as after cumc_initial_update
- * and nsteps cumc_rungekutta calls. Supported: CUMC_FP64, CUMC_CARTESIAN,
- * models NONE and RIEMANN (CUMC_ERR_CONFIG otherwise). */
+ * and nsteps cumc_rungekutta calls. Supported: CUMC_FP64 on every coordinate
+ * system (the geometric flux, CT and source terms included), models NONE
+ * and RIEMANN (CUMC_ERR_CONFIG otherwise). */
 #define CUMC_OBJ_MAGNETIC 1
 #define CUMC_OBJ_KINETIC  2
 #define CUMC_OBJ_LINEAR   3

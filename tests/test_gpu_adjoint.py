@@ -69,10 +69,18 @@ def generic_box(n, recon=N.PPMC, flags=(0, 0, 0, 0, 0, 0), seed=1):
 
 
 def _dv(prob):
+    """cell volumes of the active cells: dx dy dz, R dR dphi dz, d(r^3)/3 d(-cos) dphi"""
     nx, ny, nz = prob.nx, prob.ny, prob.nz
-    dx = np.diff(prob.xf)[2:nx + 2]
-    dy = np.diff(prob.yf)[2:ny + 2]
-    dz = np.diff(prob.zf)[2:nz + 2]
+    # face arrays hold faces -3..n+3: cell j (1..n) spans f[j+2] .. f[j+3]
+    xm, xp = prob.xf[3:nx + 3], prob.xf[4:nx + 4]
+    dx = xp - xm
+    dy = prob.yf[4:ny + 4] - prob.yf[3:ny + 3]
+    dz = prob.zf[4:nz + 4] - prob.zf[3:nz + 3]
+    if prob.coordinate == N.CYLINDRICAL:
+        dx = 0.5 * (xp + xm) * dx
+    elif prob.coordinate == N.SPHERICAL:
+        dx = (xp ** 3 - xm ** 3) / 3.0
+        dy = np.cos(prob.yf[3:ny + 3]) - np.cos(prob.yf[4:ny + 4])
     return dz[:, None, None] * dy[None, :, None] * dx[None, None, :]
 
 
@@ -170,6 +178,18 @@ def test_adjoint_vs_tangent_nonperiodic_boundaries(flags):
     prob = generic_box(10, flags=flags)
     w = np.random.default_rng(7).uniform(-1, 1, prob.prim.shape)
     _check_tangent(prob, 2, 1, N.OBJ_LINEAR, weights=w)
+
+
+@pytest.mark.parametrize("coord,kind,recon", [(N.CYLINDRICAL, N.OBJ_LINEAR, N.PPMC),
+                                               (N.SPHERICAL, N.OBJ_LINEAR, N.PPMC),
+                                               (N.CYLINDRICAL, N.OBJ_MAGNETIC, N.TVDMM),
+                                               (N.SPHERICAL, N.OBJ_KINETIC, N.PPMC)])
+def test_adjoint_vs_tangent_curvilinear(coord, kind, recon):
+    """flux-difference and CT factors and GEOM_SOURCE (added 8 times) of the
+    cylindrical and spherical grids"""
+    prob = P.shell(coord, 10, 8, 6, recon=recon)
+    w = np.random.default_rng(9).uniform(-1, 1, prob.prim.shape) if kind == N.OBJ_LINEAR else None
+    _check_tangent(prob, 2, 1, kind, weights=w)
 
 
 def _density(st, prob, kind):

@@ -44,6 +44,8 @@ SMALL = [
     ("orszag_tang_tvd", lambda: P.orszag_tang(12, recon=N.TVDMM)),
     ("torus_small", lambda: P.torus(24, 16, 8)),
     ("torus_small_q1_once", lambda: P.torus(20, 12, 6, geom_source_repeat=1)),
+    ("cylindrical_shell", lambda: P.shell(N.CYLINDRICAL, 16, 12, 10)),
+    ("spherical_shell", lambda: P.shell(N.SPHERICAL, 14, 12, 10)),
 ]
 
 
