@@ -72,3 +72,18 @@ def test_mixed_advance_equals_host_loop():
     y.advance(5)
     assert x.global_time == y.global_time
     assert np.array_equal(x.download()["cons"], y.download()["cons"])
+
+
+@pytest.mark.parametrize("coord", [N.CYLINDRICAL, N.SPHERICAL])
+def test_curvilinear_shell_mixed_vs_fp64(coord):
+    """geometric flux, CT and source terms of the mixed path on the smooth
+    shells, with the FP64 run's dt sequence replayed"""
+    a = _run(P.shell(coord, 24, 20, 16), N.FP64, steps=0)
+    dts = [a.step() for _ in range(10)]
+    b = _run(P.shell(coord, 24, 20, 16), N.MIXED, steps=0)
+    for dt in dts:
+        b.rungekutta(dt)
+    db = b.download()
+    assert np.all(np.isfinite(db["cons"][3:-3, 3:-3, 3:-3]))
+    rel = rel_l1_interior(db, a.download())
+    assert rel[0] <= RHO_L1_TOL, rel
