@@ -72,7 +72,9 @@ EXPORTS = [
     "cumc_initial_update", "cumc_finddt", "cumc_rungekutta", "cumc_spatial", "cumc_download_lrk",
     "cumc_divb", "cumc_advance", "cumc_get_stream", "cumc_profile", "cumc_profile_read",
     "cumc_launch_count", "cumc_cfl_dt_static", "cumc_cfl_dt_static_error", "cumc_adjoint_run",
+    "cumc_snapshot_async", "cumc_snapshot_wait", "cumc_restore_state",
 ]
+STATE_ARRAYS = 17
 
 
 def load(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -104,6 +106,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                                                                    c_void_p]),
         "cumc_cfl_dt_static_error": (c_char_p, []),
         "cumc_adjoint_run": (c_int, [c_void_p, c_int, c_int, c_int, dp, dp, dp, dp, dp, dp]),
+        "cumc_snapshot_async": (c_int, [c_void_p, dp]),
+        "cumc_snapshot_wait": (c_int, [c_void_p]),
+        "cumc_restore_state": (c_int, [c_void_p, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

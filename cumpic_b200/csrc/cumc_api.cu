@@ -86,6 +86,10 @@ struct cumc_ctx {
     double* const* tape = nullptr;  // adjoint: 3 x 8 arrays receiving each stage's combine output
     void* adj_slab = nullptr;       // adjoint scratch, kept between runs
     size_t adj_slab_bytes = 0;
+    double* snap_dev = nullptr;            // snapshot staging slab (17 state arrays)
+    cudaStream_t snap_stream = nullptr;    // device -> host copies of snapshots
+    cudaEvent_t snap_taken = nullptr, snap_done = nullptr;
+    bool snap_pending = false;
 
     int fail(int code, const char* fmt, ...) {
         char buf[512];
@@ -730,6 +734,12 @@ int cumc_free(cumc_ctx* c) {
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     for (void* p : c->allocs) cudaFree(p);
     if (c->adj_slab) cudaFree(c->adj_slab);
+    if (c->snap_stream) {
+        cudaStreamSynchronize(c->snap_stream);
+        cudaStreamDestroy(c->snap_stream);
+    }
+    if (c->snap_taken) cudaEventDestroy(c->snap_taken);
+    if (c->snap_done) cudaEventDestroy(c->snap_done);
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1387,4 +1397,71 @@ extern "C" int cumc_adjoint_run(cumc_ctx* c, int nsteps, int checkpoint_every, i
                                grad_prim, grad_eps);
     c->tape = nullptr;
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Snapshots and exact restart. The reference writes prim and eps
+// (solver/dataio.f90:7-331) and cannot restart; here the whole state (the 17
+// arrays a step reads: cons, w, bcell, eps) goes to the host, so that a
+// context restored from it continues bit for bit. The copy out overlaps the
+// following steps: the state is first copied to a device staging slab on the
+// context's stream, then to the host on a stream of its own.
+// ---------------------------------------------------------------------------
+namespace {
+int snapshot_setup(cumc_ctx* c) {
+    if (c->snap_dev) return CUMC_OK;
+    int rc = dalloc(c, &c->snap_dev, STATE_ARRAYS * (size_t)c->box.count());
+    if (rc != CUMC_OK) return rc;
+    CUMC_CHECK(cudaStreamCreateWithFlags(&c->snap_stream, cudaStreamNonBlocking));
+    CUMC_CHECK(cudaEventCreateWithFlags(&c->snap_taken, cudaEventDisableTiming));
+    CUMC_CHECK(cudaEventCreateWithFlags(&c->snap_done, cudaEventDisableTiming));
+    return CUMC_OK;
+}
+}  // namespace
+
+extern "C" int cumc_snapshot_async(cumc_ctx* c, double* host_state) {
+    int rc = check_ready(c);
+    if (rc != CUMC_OK) return rc;
+    if (c->mixed) return c->fail(CUMC_ERR_CONFIG, "snapshots cover CUMC_FP64");
+    if (!host_state) return c->fail(CUMC_ERR_ARG, "null host buffer");
+    if ((rc = snapshot_setup(c)) != CUMC_OK) return rc;
+    const size_t NT = (size_t)c->box.count();
+    // the slab is reused: the previous snapshot's copy out must have read it
+    if (c->snap_pending) CUMC_CHECK(cudaStreamWaitEvent(c->stream, c->snap_done, 0));
+    StateSet s = live_state(c);
+    for (int i = 0; i < STATE_ARRAYS; ++i)
+        CUMC_CHECK(cudaMemcpyAsync(c->snap_dev + i * NT, *s.all(i), NT * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   c->stream));
+    CUMC_CHECK(cudaEventRecord(c->snap_taken, c->stream));
+    CUMC_CHECK(cudaStreamWaitEvent(c->snap_stream, c->snap_taken, 0));
+    CUMC_CHECK(cudaMemcpyAsync(host_state, c->snap_dev, STATE_ARRAYS * NT * sizeof(double), cudaMemcpyDeviceToHost,
+                               c->snap_stream));
+    CUMC_CHECK(cudaEventRecord(c->snap_done, c->snap_stream));
+    c->snap_pending = true;
+    return CUMC_OK;
+}
+
+extern "C" int cumc_snapshot_wait(cumc_ctx* c) {
+    if (!c) return CUMC_ERR_ARG;
+    if (c->snap_pending) {
+        CUMC_CHECK(cudaEventSynchronize(c->snap_done));
+        c->snap_pending = false;
+    }
+    return CUMC_OK;
+}
+
+extern "C" int cumc_restore_state(cumc_ctx* c, const double* host_state) {
+    if (!c || !host_state) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
+    if (c->mixed) return c->fail(CUMC_ERR_CONFIG, "snapshots cover CUMC_FP64");
+    int rc = cumc_snapshot_wait(c);  // the staging slab and stream are quiet
+    if (rc != CUMC_OK) return rc;
+    const size_t NT = (size_t)c->box.count();
+    StateSet s = live_state(c);
+    for (int i = 0; i < STATE_ARRAYS; ++i)
+        CUMC_CHECK(cudaMemcpyAsync(*s.all(i), host_state + i * NT, NT * sizeof(double), cudaMemcpyHostToDevice,
+                                   c->stream));
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    c->uploaded = true;
+    c->ready = true;
+    return sync_status(c);
 }

@@ -150,6 +150,58 @@ class CUMC3D:
         self.global_time = float(np.sum(dt_out))
         return {"J": J.value, "grad_prim": gp, "grad_eps": ge, "dts": dt_out}
 
+    # -- snapshots and restart -------------------------------------------------
+    def state_buffer(self) -> np.ndarray:
+        """a host buffer for one state (STATE_ARRAYS x shape doubles), pinned
+        when torch can provide pinned memory, so that the copy out overlaps"""
+        shape = (N.STATE_ARRAYS,) + self.shape
+        try:
+            import torch
+            return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+        except Exception:
+            return np.empty(shape)
+
+    def snapshot_async(self, host_state: np.ndarray):
+        """cumc_snapshot_async: the current state is copied out to host_state
+        while the following steps run; host_state stays untouched until
+        snapshot_wait returns"""
+        if host_state.shape != (N.STATE_ARRAYS,) + self.shape or host_state.dtype != np.float64 or \
+                not host_state.flags.c_contiguous:
+            raise ValueError("host_state must be a C-contiguous float64 array of shape (17,) + shape")
+        self._snap = host_state
+        self._snap_meta = (self.global_time, self.n_step)
+        self._check(self._lib.cumc_snapshot_async(self._h, _dp(host_state)))
+
+    def snapshot_wait(self) -> tuple[float, int]:
+        """cumc_snapshot_wait; returns the (time, step) the snapshot was taken at"""
+        self._check(self._lib.cumc_snapshot_wait(self._h))
+        return getattr(self, "_snap_meta", (self.global_time, self.n_step))
+
+    def restore_state(self, host_state: np.ndarray, global_time: float = 0.0, n_step: int = 0):
+        """cumc_restore_state: continue from a state taken by snapshot_async"""
+        st = np.ascontiguousarray(host_state, dtype=np.float64)
+        if st.shape != (N.STATE_ARRAYS,) + self.shape:
+            raise ValueError("the state does not match this grid")
+        self._check(self._lib.cumc_restore_state(self._h, _dp(st)))
+        self.global_time, self.n_step = float(global_time), int(n_step)
+
+    def save_snapshot(self, path: str):
+        """the state now, with time and step, to a snapshot file"""
+        from . import snapshot
+        buf = self.state_buffer()
+        self.snapshot_async(buf)
+        t, n = self.snapshot_wait()
+        snapshot.write(path, self.problem, buf, t, n)
+
+    def load_snapshot(self, path: str):
+        """continue from a snapshot file of this grid"""
+        from . import snapshot
+        s = snapshot.read(path)
+        p = self.problem
+        if (s["nx"], s["ny"], s["nz"], s["coordinate"]) != (p.nx, p.ny, p.nz, p.coordinate):
+            raise ValueError(f"{path}: the snapshot's grid differs from this context's")
+        self.restore_state(snapshot.datasets_to_state(s["datasets"]), s["time"], s["step"])
+
     # -- instrumentation -----------------------------------------------------
     def stream_handle(self) -> int:
         s = ctypes.c_void_p()

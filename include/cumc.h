@@ -176,6 +176,28 @@ int cumc_profile_read(cumc_ctx* ctx, int which, int* launches, double* ms);
 /* Number of kernel launches the library issued since cumc_init. */
 int cumc_launch_count(cumc_ctx* ctx, long long* count);
 
+/* Snapshot and exact restart of the FP64 state. Replace the reference's
+ * output step print_hydroprofile (solver/dataio.f90:7-77, HDF5 prim and eps
+ * only, no restart). The state is the 17 arrays a step reads, each
+ * (nx+6)(ny+6)(nz+6) doubles in the index order of the prim layout without
+ * its field index (x fastest): cons 1-8, prim 1-5 (rho, vx, vy, vz, p),
+ * bcell 1-3, eps; CUMC_STATE_ARRAYS of them back to back.
+ *
+ * cumc_snapshot_async copies the current state (after cumc_initial_update or
+ * a step) to a device staging slab on the context's stream, then to
+ * host_state on a second stream, and returns at once: the steps issued next
+ * overlap the copy out and do not change what it delivers. host_state should
+ * be pinned for the copy to be asynchronous, and must stay untouched until
+ * cumc_snapshot_wait returns. A second snapshot waits (on the device) for the
+ * first one's copy out. The staging slab is allocated on the first call.
+ * cumc_restore_state uploads such a state; the context then continues
+ * exactly as the one that took it (no cumc_initial_update needed). Both
+ * return CUMC_ERR_CONFIG for CUMC_MIXED. */
+#define CUMC_STATE_ARRAYS 17
+int cumc_snapshot_async(cumc_ctx* ctx, double* host_state);
+int cumc_snapshot_wait(cumc_ctx* ctx);
+int cumc_restore_state(cumc_ctx* ctx, const double* host_state);
+
 /* Discrete adjoint of the FP64 path. No counterpart in the reference, which
  * has no derivatives; it is the new entry point cumc_adjoint_run of the hot
  * path's drop-in boundary.
