@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-snapshot", action="store_true")
     ap.add_argument("--adjoint-check", action="store_true",
                     help="also run the full finite-difference check of the adjoint (128^3, 200 steps, 16 directions)")
     ap.add_argument("--all-configs", action="store_true",
@@ -283,6 +284,53 @@ def mixed_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> d
         out["vs_fp64"][f"bscale_{bscale:g}"] = {"rel_l1": {k: rel[q] for q, k in enumerate(names)},
                                                 "max_divb_norm": res[NN.MIXED][1]}
     return out
+
+
+def snapshot_section(n: int, steps: int = 20) -> dict:
+    """cumc_snapshot_async on the workload: the steps alone, the same steps
+    with a snapshot of the whole state (17 arrays) taken before them and
+    copied out to pinned host memory while they run, and the copy out alone"""
+    import torch
+    from cumpic_b200 import problems as P
+    from cumpic_b200.solver import CUMC3D
+    sim = CUMC3D(P.orszag_tang(n))
+    sim.upload()
+    sim.initial_update()
+    sim.advance(3)
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    buf = sim.state_buffer()
+    sim.snapshot_async(buf)  # first call: staging slab and stream
+    sim.snapshot_wait()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sim.advance(steps)
+    e1.record(stream)
+    e1.synchronize()
+    plain = e0.elapsed_time(e1)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    sim.snapshot_async(buf)
+    sim.advance(steps)
+    e1.record(stream)
+    e1.synchronize()
+    with_snap = e0.elapsed_time(e1)
+    sim.snapshot_wait()
+    wall = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sim.snapshot_async(buf)
+    sim.snapshot_wait()
+    alone = time.perf_counter() - t0
+    pinned = False
+    try:
+        pinned = bool(torch.from_numpy(buf).is_pinned())
+    except Exception:
+        pass
+    sim.close()
+    return {"bytes": int(buf.nbytes), "pinned_host": pinned, "steps": steps, "ms_steps": plain,
+            "ms_steps_with_snapshot": with_snap, "overhead_ms": with_snap - plain,
+            "ms_wall_snapshot_and_steps": 1e3 * wall, "ms_copy_out_alone": 1e3 * alone,
+            "what": "steps timed with CUDA events on the context stream; the copy out runs on its own stream"}
 
 
 def adjoint_section(n: int = 128, steps: int = 200, ckpt: int = 20) -> dict:
@@ -568,6 +616,8 @@ def run_ours(args, world, rank, local):
     sim.close()
     if world == 1 and not args.no_mixed:
         line["mixed"] = mixed_section(n, args.steps, args.warmup, ms_max / args.steps)
+    if world == 1 and not args.no_snapshot:
+        line["snapshot"] = snapshot_section(n)
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_section()
         if args.adjoint_check:

@@ -73,7 +73,9 @@ EXPORTS = [
     "cumc_divb", "cumc_advance", "cumc_get_stream", "cumc_profile", "cumc_profile_read",
     "cumc_launch_count", "cumc_cfl_dt_static", "cumc_cfl_dt_static_error", "cumc_adjoint_run",
     "cumc_snapshot_async", "cumc_snapshot_wait", "cumc_restore_state",
+    "cumc_rk_stage", "cumc_halo_doubles", "cumc_halo_pack", "cumc_halo_unpack",
 ]
+BC_EXCHANGE = -1
 STATE_ARRAYS = 17
 
 
@@ -106,6 +108,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                                                                    c_void_p]),
         "cumc_cfl_dt_static_error": (c_char_p, []),
         "cumc_adjoint_run": (c_int, [c_void_p, c_int, c_int, c_int, dp, dp, dp, dp, dp, dp]),
+        "cumc_rk_stage": (c_int, [c_void_p, c_int, c_double]),
+        "cumc_halo_doubles": (c_int, [c_void_p, POINTER(c_longlong)]),
+        "cumc_halo_pack": (c_int, [c_void_p, c_int, c_void_p]),
+        "cumc_halo_unpack": (c_int, [c_void_p, c_int, c_void_p]),
         "cumc_snapshot_async": (c_int, [c_void_p, dp]),
         "cumc_snapshot_wait": (c_int, [c_void_p]),
         "cumc_restore_state": (c_int, [c_void_p, dp]),

@@ -86,6 +86,9 @@ struct cumc_ctx {
     double* const* tape = nullptr;  // adjoint: 3 x 8 arrays receiving each stage's combine output
     void* adj_slab = nullptr;       // adjoint scratch, kept between runs
     size_t adj_slab_bytes = 0;
+    int next_stage = 1;    // cumc_rk_stage: the stage due next
+    int bf_set = 0;        // U[bf_set] holds the current face fields (the last stage's output)
+    bool exchange = false;  // a z face is CUMC_BC_EXCHANGE
     double* snap_dev = nullptr;            // snapshot staging slab (17 state arrays)
     cudaStream_t snap_stream = nullptr;    // device -> host copies of snapshots
     cudaEvent_t snap_taken = nullptr, snap_done = nullptr;
@@ -492,6 +495,24 @@ void loop_step(cumc_ctx* c, double t_end) {
     launch(c, -1, 1, 1, k_advance_time, k);
 }
 
+// halo planes of a z face: the 11 arrays a neighbouring slab reads in its
+// ghost planes (w, bcell, eps, and the face fields Bx, By), three planes from
+// plane l0, each plane whole (x and y ghosts included)
+constexpr int HALO_ARRAYS = 11;
+struct HaloArgs {
+    double* f[HALO_ARRAYS];
+};
+__global__ void __launch_bounds__(256) k_halo_copy(Box b, HaloArgs a, int l0, double* buf, int to_buf) {
+    const long long plane = (long long)b.SX * b.SY;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= HALO_ARRAYS * 3 * plane) return;
+    const int q = (int)(t / (3 * plane));
+    const long long r = t % (3 * plane);
+    const long long at = (long long)(l0 + 2) * plane + r;  // plane l0 + r/plane (Box::idx), cell r%plane
+    if (to_buf) buf[t] = a.f[q][at];
+    else a.f[q][at] = buf[t];
+}
+
 int check_ready(cumc_ctx* c) {
     if (!c) return CUMC_ERR_ARG;
     if (!c->ready) return c->fail(CUMC_ERR_STATE, "cumc_initial_update must run after cumc_upload_state first");
@@ -525,7 +546,12 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     if (cfg->precision != CUMC_FP64 && cfg->precision != CUMC_MIXED) return bad("precision must be CUMC_FP64 or CUMC_MIXED");
     if (cfg->model < 0 || cfg->model > 3) return bad("unknown model id");
     for (int i = 0; i < 6; ++i)
-        if (cfg->boundary_flag[i] < 0 || cfg->boundary_flag[i] > 4) return bad("boundary_flag entries must be 0..4");
+        if ((cfg->boundary_flag[i] < 0 || cfg->boundary_flag[i] > 4) &&
+            !(i >= 4 && cfg->boundary_flag[i] == CUMC_BC_EXCHANGE))
+            return bad("boundary_flag entries must be 0..4 (z faces: or CUMC_BC_EXCHANGE)");
+    if ((cfg->boundary_flag[4] == CUMC_BC_EXCHANGE || cfg->boundary_flag[5] == CUMC_BC_EXCHANGE) &&
+        cfg->precision != CUMC_FP64)
+        return bad("CUMC_BC_EXCHANGE faces need CUMC_FP64");
     if (cfg->boundary_flag[0] == 4 || cfg->boundary_flag[1] == 4)
         return bad("equatorial symmetry is not allowed for the x-boundary (solver/setup.f90:147-151)");
     if (cfg->boundary_flag[4] == 3 || cfg->boundary_flag[5] == 3)
@@ -554,6 +580,7 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     c->ggas = cfg->ggas;
     c->cfl = cfg->cfl;
     for (int i = 0; i < 6; ++i) c->flag[i] = cfg->boundary_flag[i];
+    c->exchange = c->flag[4] == CUMC_BC_EXCHANGE || c->flag[5] == CUMC_BC_EXCHANGE;
     // bfac tables (solver/setup.f90:129-230)
     for (int s = 0; s < 6; ++s)
         for (int q = 0; q < 8; ++q) c->fac[s][q] = 1;
@@ -847,6 +874,8 @@ int cumc_initial_update(cumc_ctx* c) {
     utop(c, c->box, c->U[c->cur], false);
     boundary(c, c->box, c->U[c->cur]);
     c->ready = true;
+    c->next_stage = 1;
+    c->bf_set = c->cur;
     return sync_status(c);
 }
 
@@ -869,10 +898,50 @@ int cumc_finddt(cumc_ctx* c, double* dt) {
 int cumc_rungekutta(cumc_ctx* c, double dt) {
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
+    if (c->exchange) return c->fail(CUMC_ERR_STATE, "a slab with CUMC_BC_EXCHANGE faces steps by cumc_rk_stage and the halo exchange");
+    if (c->next_stage != 1) return c->fail(CUMC_ERR_STATE, "cumc_rk_stage left a step unfinished");
     launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
     rk_step(c, c->box);
     return sync_status(c);
 }
+
+int cumc_rk_stage(cumc_ctx* c, int stage, double dt) {
+    int rc = check_ready(c);
+    if (rc != CUMC_OK) return rc;
+    if (stage != c->next_stage) return c->fail(CUMC_ERR_STATE, "stage %d called where stage %d is due", stage, c->next_stage);
+    if (stage == 1) launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
+    run_stage(c, c->box, stage);
+    c->next_stage = stage == 3 ? 1 : stage + 1;
+    c->bf_set = stage == 3 ? c->cur : 1 - c->cur;
+    return sync_status(c);
+}
+
+int cumc_halo_doubles(cumc_ctx* c, long long* n) {
+    if (!c || !n) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
+    *n = (long long)HALO_ARRAYS * 3 * c->box.SX * c->box.SY;
+    return CUMC_OK;
+}
+
+static int halo_copy(cumc_ctx* c, int side, double* buf, bool pack) {
+    int rc = check_ready(c);
+    if (rc != CUMC_OK) return rc;
+    if (c->mixed) return c->fail(CUMC_ERR_CONFIG, "the halo exchange covers CUMC_FP64");
+    if ((side != 0 && side != 1) || !buf) return c->fail(CUMC_ERR_ARG, "side must be 0 (z-in) or 1 (z-out), buffer non-null");
+    const Box& b = c->box;
+    HaloArgs a;
+    for (int q = 0; q < 5; ++q) a.f[q] = c->w[q];
+    for (int q = 0; q < 3; ++q) a.f[5 + q] = c->bc[q];
+    a.f[8] = c->eps;
+    a.f[9] = c->U[c->bf_set][IBX];
+    a.f[10] = c->U[c->bf_set][IBY];
+    // pack: the three active planes next to the face; unpack: its three ghost planes
+    const int l0 = pack ? (side == 0 ? 1 : b.nz - 2) : (side == 0 ? -2 : b.nz + 1);
+    launch(c, -1, (long long)HALO_ARRAYS * 3 * b.SX * b.SY, 256, k_halo_copy, b, a, l0, buf, pack ? 1 : 0);
+    return sync_status(c);
+}
+
+int cumc_halo_pack(cumc_ctx* c, int side, double* buf) { return halo_copy(c, side, buf, true); }
+int cumc_halo_unpack(cumc_ctx* c, int side, const double* buf) { return halo_copy(c, side, const_cast<double*>(buf), false); }
 
 int cumc_spatial(cumc_ctx* c) {
     int rc = check_ready(c);
@@ -933,6 +1002,8 @@ int cumc_divb(cumc_ctx* c, double* maxdb_signed, double* maxabs_norm) {
 int cumc_advance(cumc_ctx* c, int nsteps, double t_end, double* t_inout, int* steps_done) {
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
+    if (c->exchange) return c->fail(CUMC_ERR_STATE, "a slab with CUMC_BC_EXCHANGE faces steps by cumc_rk_stage and the halo exchange");
+    if (c->next_stage != 1) return c->fail(CUMC_ERR_STATE, "cumc_rk_stage left a step unfinished");
     if (nsteps < 0 || !t_inout) return c->fail(CUMC_ERR_ARG, "nsteps must be >= 0 and t_inout non-null");
     launch(c, -1, 1, 1, k_set_scalar, c->scal + 1, *t_inout);
     CUMC_CHECK(cudaMemsetAsync(c->ints, 0, 2 * sizeof(int), c->stream));
@@ -1388,8 +1459,8 @@ extern "C" int cumc_adjoint_run(cumc_ctx* c, int nsteps, int checkpoint_every, i
                                 const double* dt_in, double* dt_out, double* J, double* grad_prim, double* grad_eps) {
     if (!c) return CUMC_ERR_ARG;
     if (!c->uploaded) return c->fail(CUMC_ERR_STATE, "cumc_upload_state must come first");
-    if (c->mixed || (c->model != CUMC_MODEL_NONE && c->model != CUMC_MODEL_RIEMANN))
-        return c->fail(CUMC_ERR_CONFIG, "the adjoint covers CUMC_FP64 with model NONE or RIEMANN");
+    if (c->mixed || c->exchange || (c->model != CUMC_MODEL_NONE && c->model != CUMC_MODEL_RIEMANN))
+        return c->fail(CUMC_ERR_CONFIG, "the adjoint covers CUMC_FP64 with model NONE or RIEMANN on one domain");
     if (nsteps < 1 || checkpoint_every < 1) return c->fail(CUMC_ERR_ARG, "nsteps and checkpoint_every must be >= 1");
     if (objective < CUMC_OBJ_MAGNETIC || objective > CUMC_OBJ_LINEAR) return c->fail(CUMC_ERR_ARG, "unknown objective");
     if (objective == CUMC_OBJ_LINEAR && !weights) return c->fail(CUMC_ERR_ARG, "CUMC_OBJ_LINEAR needs weights");
@@ -1463,5 +1534,7 @@ extern "C" int cumc_restore_state(cumc_ctx* c, const double* host_state) {
     CUMC_CHECK(cudaStreamSynchronize(c->stream));
     c->uploaded = true;
     c->ready = true;
+    c->next_stage = 1;
+    c->bf_set = c->cur;
     return sync_status(c);
 }

@@ -12,6 +12,7 @@
 // The reference's intermediates primL/primR/consL/consR/fluxL/fluxR/l_rk/sc/
 // ecell never reach HBM here; only the face fluxes and edge EMFs do.
 #pragma once
+#include "../../include/cumc.h"
 #include "cumc_device.cuh"
 
 namespace cumc {
@@ -514,66 +515,70 @@ __global__ void __launch_bounds__(256) k_boundary(Box b, BoundArgsT<R> a) {
     const bool gx = gmap(j, b.nx, a.flag[0], a.flag[1], sj, dj);
     const bool gy = gmap(k, b.ny, a.flag[2], a.flag[3], sk, dk);
     const bool gz = gmap(l, b.nz, a.flag[4], a.flag[5], sl, dl);
-    // parity sign of equation q across the mapped directions (reflecting
-    // boundaries only: flags 0 and 1 copy without sign)
-    // parity sign of equation q across the mapped directions (bfac is 1
-    // except at reflecting faces, flags >= 2)
-    auto sgn = [&](int q) -> int {
-        int s = 1;
-        if (gx && a.flag[dj] >= 2) s *= a.fac[dj][q];
-        if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][q];
-        if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][q];
-        return s;
-    };
-    const int src = b.idx(sj, sk, sl);
-    R w[4];
+    // z ghost planes of a face shared with a neighbouring slab come from the
+    // halo exchange; only Bz on the face l = 0 itself, a live face whose
+    // x/y ghost copies are local, is filled here
+    const bool exch = (l < 1 && a.flag[4] == CUMC_BC_EXCHANGE) || (l > b.nz && a.flag[5] == CUMC_BC_EXCHANGE);
+    if (!exch) {
+        // parity sign of equation q across the mapped directions (bfac is 1
+        // except at reflecting faces, flags >= 2)
+        auto sgn = [&](int q) -> int {
+            int s = 1;
+            if (gx && a.flag[dj] >= 2) s *= a.fac[dj][q];
+            if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][q];
+            if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][q];
+            return s;
+        };
+        const int src = b.idx(sj, sk, sl);
+        R w[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const R v = a.w[q][src];
-        w[q] = sgn(q) == 1 ? v : -v;
-    }
+        for (int q = 0; q < 4; ++q) {
+            const R v = a.w[q][src];
+            w[q] = sgn(q) == 1 ? v : -v;
+        }
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        const R v = a.bc[q][src];
-        a.bc[q][i] = sgn(IBX + q) == 1 ? v : -v;
-    }
-    // torus ghost clamps (CUSTOM_BOUNDARY) act after all copies
-    if (MODEL == 2 || MODEL == 3) {
-        if (j < 1) w[1] = fmin(w[1], R(0));
-        if (j > b.nx) w[1] = fmax(w[1], R(0));
-    }
-    if (MODEL == 3) {
-        if (l < 1) w[3] = fmin(w[3], R(0));
-        if (l > b.nz) w[3] = fmax(w[3], R(0));
-    }
+        for (int q = 0; q < 3; ++q) {
+            const R v = a.bc[q][src];
+            a.bc[q][i] = sgn(IBX + q) == 1 ? v : -v;
+        }
+        // torus ghost clamps (CUSTOM_BOUNDARY) act after all copies
+        if (MODEL == 2 || MODEL == 3) {
+            if (j < 1) w[1] = fmin(w[1], R(0));
+            if (j > b.nx) w[1] = fmax(w[1], R(0));
+        }
+        if (MODEL == 3) {
+            if (l < 1) w[3] = fmin(w[3], R(0));
+            if (l > b.nz) w[3] = fmax(w[3], R(0));
+        }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) a.w[q][i] = w[q];
-    if (a.eps) {
-        // eps: BOUNDARY1D with even parity; its y-outer branch keys on flag(3)
-        int ej = j, ek = k, el = l, dd;
-        gmap(j, b.nx, a.flag[0], a.flag[1], ej, dd);
-        gmap(k, b.ny, a.flag[2], a.eps_yout, ek, dd);
-        gmap(l, b.nz, a.flag[4], a.flag[5], el, dd);
-        const double e = a.eps[b.idx(ej, ek, el)];
-        a.eps[i] = e;
-        a.w[4][i] = (R)(((double)w[0] * e) * (a.ggas - 1.0));  // UPDATE on the ghost
-    } else {
-        a.w[4][i] = a.w[4][src];  // pressure is even under every map
-    }
-    // tangential face fields
-    if (j >= 0 && j <= b.nx && (gy || gz)) {  // Bx: map y and z only
-        int s = 1;
-        if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][IBX];
-        if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][IBX];
-        const R v = a.bf[0][b.idx(j, sk, sl)];
-        a.bf[0][i] = s == 1 ? v : -v;
-    }
-    if (k >= 0 && k <= b.ny && (gx || gz)) {  // By: map x and z only
-        int s = 1;
-        if (gx && a.flag[dj] >= 2) s *= a.fac[dj][IBY];
-        if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][IBY];
-        const R v = a.bf[1][b.idx(sj, k, sl)];
-        a.bf[1][i] = s == 1 ? v : -v;
+        for (int q = 0; q < 4; ++q) a.w[q][i] = w[q];
+        if (a.eps) {
+            // eps: BOUNDARY1D with even parity; its y-outer branch keys on flag(3)
+            int ej = j, ek = k, el = l, dd;
+            gmap(j, b.nx, a.flag[0], a.flag[1], ej, dd);
+            gmap(k, b.ny, a.flag[2], a.eps_yout, ek, dd);
+            gmap(l, b.nz, a.flag[4], a.flag[5], el, dd);
+            const double e = a.eps[b.idx(ej, ek, el)];
+            a.eps[i] = e;
+            a.w[4][i] = (R)(((double)w[0] * e) * (a.ggas - 1.0));  // UPDATE on the ghost
+        } else {
+            a.w[4][i] = a.w[4][src];  // pressure is even under every map
+        }
+        // tangential face fields
+        if (j >= 0 && j <= b.nx && (gy || gz)) {  // Bx: map y and z only
+            int s = 1;
+            if (gy && a.flag[2 + dk] >= 2) s *= a.fac[2 + dk][IBX];
+            if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][IBX];
+            const R v = a.bf[0][b.idx(j, sk, sl)];
+            a.bf[0][i] = s == 1 ? v : -v;
+        }
+        if (k >= 0 && k <= b.ny && (gx || gz)) {  // By: map x and z only
+            int s = 1;
+            if (gx && a.flag[dj] >= 2) s *= a.fac[dj][IBY];
+            if (gz && a.flag[4 + dl] >= 2) s *= a.fac[4 + dl][IBY];
+            const R v = a.bf[1][b.idx(sj, k, sl)];
+            a.bf[1][i] = s == 1 ? v : -v;
+        }
     }
     if (l >= 0 && l <= b.nz && (gx || gy)) {  // Bz: map x and y only
         int s = 1;

@@ -150,6 +150,11 @@ class CUMC3D:
         self.global_time = float(np.sum(dt_out))
         return {"J": J.value, "grad_prim": gp, "grad_eps": ge, "dts": dt_out}
 
+    def rk_stage(self, stage: int, dt: float):
+        """cumc_rk_stage: one stage of RUNGEKUTTA (1, 2, 3 in order; dt read
+        at stage 1), for slabs that exchange halos between stages"""
+        self._check(self._lib.cumc_rk_stage(self._h, int(stage), float(dt)))
+
     # -- snapshots and restart -------------------------------------------------
     def state_buffer(self) -> np.ndarray:
         """a host buffer for one state (STATE_ARRAYS x shape doubles), pinned

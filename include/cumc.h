@@ -76,7 +76,8 @@ typedef struct cumc_config {
     int coordinate;          /* CUMC_CARTESIAN / CUMC_CYLINDRICAL / CUMC_SPHERICAL */
     int boundary_flag[6];    /* x-in, x-out, y-in, y-out, z-in, z-out: 0 periodic,
                                 1 outflow, 2 reflect, 3 axis, 4 equatorial
-                                (solver/definition.f90:74-87)                       */
+                                (solver/definition.f90:74-87); z faces may also be
+                                CUMC_BC_EXCHANGE (a neighbouring slab's face)     */
     double ggas;             /* adiabatic index (model/<m>/src/defs.f90:14)        */
     double cfl;              /* Courant number (solver/definition.f90:116)        */
     int recon;               /* CUMC_PPMC or CUMC_TVDMM                            */
@@ -175,6 +176,31 @@ int cumc_profile_read(cumc_ctx* ctx, int which, int* launches, double* ms);
 
 /* Number of kernel launches the library issued since cumc_init. */
 int cumc_launch_count(cumc_ctx* ctx, long long* count);
+
+/* z-slab decomposition: the halo exchange between slabs (replaces the MPI
+ * path of solver/mpi.f90:255-501, MPI_BOUNDARYP_Z / MPI_BOUNDARY_Z, and the
+ * internal faces of solver/boundary.f90:332-336,663-667). A z face whose
+ * boundary_flag is CUMC_BC_EXCHANGE is shared with a neighbouring slab: the
+ * boundary fill leaves its three ghost planes alone (except the face field
+ * Bz on the face itself, which CT computes on both sides) and the caller
+ * fills them from the neighbour after cumc_initial_update and after every
+ * stage. A slab steps by cumc_rk_stage(ctx, 1..3, dt) (dt read at stage 1;
+ * the three stages of RUNGEKUTTA, solver/rungekutta.f90:38-134, each with
+ * its conversions and boundary fill); cumc_rungekutta, cumc_advance and
+ * cumc_adjoint_run refuse such a context. cumc_halo_pack(ctx, side, buf)
+ * copies the three active planes next to face `side` (0: z-in, planes 1..3;
+ * 1: z-out, planes nz-2..nz) of w (5), bcell (3), eps and the face fields
+ * Bx, By into the device buffer buf (cumc_halo_doubles doubles: 11 arrays
+ * x 3 planes x (nx+6)(ny+6)); cumc_halo_unpack(ctx, side, buf) writes a
+ * neighbour's packed planes into the ghost planes of face `side` (0: planes
+ * -2..0 from the z-in neighbour's side-1 pack; 1: planes nz+1..nz+3 from the
+ * z-out neighbour's side-0 pack). Both are enqueued on the context's stream
+ * (cumc_get_stream). FP64 only. */
+#define CUMC_BC_EXCHANGE (-1)
+int cumc_rk_stage(cumc_ctx* ctx, int stage, double dt);
+int cumc_halo_doubles(cumc_ctx* ctx, long long* n);
+int cumc_halo_pack(cumc_ctx* ctx, int side, double* buf);
+int cumc_halo_unpack(cumc_ctx* ctx, int side, const double* buf);
 
 /* Snapshot and exact restart of the FP64 state. Replace the reference's
  * output step print_hydroprofile (solver/dataio.f90:7-77, HDF5 prim and eps
