@@ -304,8 +304,11 @@ __global__ void __launch_bounds__(256) k_combine(Box b, Tabs T, Prim pr, FaceFlu
 
 // face fields of RK stage STAGE. Each thread reads u0, uc and writes ud at its
 // own index only, so ud may alias u0 or uc.
+// (8 blocks of 256 per SM: these two kernels wait on memory, and a full SM
+// of warps hides more of it than 5 blocks without spills: 1.44 -> 1.23 ms and
+// 0.47 -> 0.36 ms at 256^3)
 template <int COORD, int STAGE>
-__global__ void __launch_bounds__(256) k_ct(Box b, Tabs T, CombineArgs a) {
+__global__ void __launch_bounds__(256, 8) k_ct(Box b, Tabs T, CombineArgs a) {
     int j, k, l, i;
     if (!box1_index(b, j, k, l, i)) return;
     double L[3];
@@ -418,7 +421,7 @@ __global__ void __launch_bounds__(256) k_utop(Box b, UtopArgs a) {
 // stage. o.u is a.ud; w, bc and eps of o are the arrays pr reads, each at the
 // thread's own index only, before the thread writes them.
 template <int COORD, int MODEL, int STAGE>
-__global__ void __launch_bounds__(256) k_combine_utop(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy, FaceFlux fz,
+__global__ void __launch_bounds__(256, 8) k_combine_utop(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy, FaceFlux fz,
                                                       CombineArgs a, UtopArgs o) {
     int j, k, l, i;
     if (!box1_index(b, j, k, l, i)) return;
