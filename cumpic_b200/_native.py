@@ -73,10 +73,15 @@ EXPORTS = [
     "cumc_divb", "cumc_advance", "cumc_get_stream", "cumc_profile", "cumc_profile_read",
     "cumc_launch_count", "cumc_cfl_dt_static", "cumc_cfl_dt_static_error", "cumc_adjoint_run",
     "cumc_snapshot_async", "cumc_snapshot_wait", "cumc_restore_state",
-    "cumc_rk_stage", "cumc_halo_doubles", "cumc_halo_pack", "cumc_halo_unpack",
+    "cumc_rk_stage", "cumc_halo_doubles", "cumc_halo_pack", "cumc_halo_unpack", "cumc_model_torus",
 ]
 BC_EXCHANGE = -1
 STATE_ARRAYS = 17
+
+
+class CumcTorusModel(ctypes.Structure):
+    _fields_ = [(n, c_double) for n in ("r_sh", "s_in", "s_max", "q_grad", "rho_max", "rho_fac", "rho_cut", "beta",
+                                        "noise")] + [("seed", ctypes.c_ulonglong)]
 
 
 def load(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -112,6 +117,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "cumc_halo_doubles": (c_int, [c_void_p, POINTER(c_longlong)]),
         "cumc_halo_pack": (c_int, [c_void_p, c_int, c_void_p]),
         "cumc_halo_unpack": (c_int, [c_void_p, c_int, c_void_p]),
+        "cumc_model_torus": (c_int, [c_void_p, POINTER(CumcTorusModel)]),
         "cumc_snapshot_async": (c_int, [c_void_p, dp]),
         "cumc_snapshot_wait": (c_int, [c_void_p]),
         "cumc_restore_state": (c_int, [c_void_p, dp]),

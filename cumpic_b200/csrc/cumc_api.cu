@@ -89,6 +89,7 @@ struct cumc_ctx {
     int next_stage = 1;    // cumc_rk_stage: the stage due next
     int bf_set = 0;        // U[bf_set] holds the current face fields (the last stage's output)
     bool exchange = false;  // a z face is CUMC_BC_EXCHANGE
+    unsigned long long* model_max = nullptr;  // cumc_model_torus: the two maxima
     double* snap_dev = nullptr;            // snapshot staging slab (17 state arrays)
     cudaStream_t snap_stream = nullptr;    // device -> host copies of snapshots
     cudaEvent_t snap_taken = nullptr, snap_done = nullptr;
@@ -493,6 +494,123 @@ void loop_step(cumc_ctx* c, double t_end) {
     launch(c, -1, 1, 1, k_clip_dt, k, t_end);
     rk_step(c, b);
     launch(c, -1, 1, 1, k_advance_time, k);
+}
+
+// ---------------------------------------------------------------------------
+// Device-side GET_MODEL of the spherical torus (model/torus_sph/src/model.f90
+// :8-284; the same construction as problems.torus on the host), written in
+// the upload layout (prim AoS, 8 values a cell, and eps) to the staging
+// buffer, so that the rest is cumc_upload_state's path.
+// ---------------------------------------------------------------------------
+struct TorusK {
+    double ggas, r_sh, s_in, q, lkep2, c_const, k_poly, rho_a, rho_max, rho_cut, beta, noise, rho_floor;
+    unsigned long long seed;
+};
+
+// equilibrium of cell (j, k) (active): rho, v_phi, p, eps
+__device__ __forceinline__ void torus_cell(const Tabs& T, const TorusK& m, int j, int k, double& rho, double& vph,
+                                           double& p, double& eps) {
+    const double r = T.ax[0].c[j];
+    const double s_eq = r * T.sinc[k];
+    const double schw = -1.0 / (r - m.r_sh);
+    double h = -schw + m.lkep2 * pow(s_eq, 2.0 - 2.0 * m.q) / (2.0 - 2.0 * m.q) + m.c_const;
+    h = fmax(h, 0.0);
+    const double rho_loc = pow(h * (m.ggas - 1.0) / m.ggas / m.k_poly, 1.0 / (m.ggas - 1.0));
+    const bool inside = rho_loc > m.rho_a && s_eq >= m.s_in;
+    rho = inside ? rho_loc : m.rho_a;
+    vph = inside ? sqrt(m.lkep2) * pow(s_eq, -m.q) * s_eq : 0.0;
+    p = m.k_poly * pow(rho, m.ggas);
+    eps = m.k_poly * pow(rho, m.ggas - 1.0) / (m.ggas - 1.0);
+}
+
+__global__ void __launch_bounds__(256) k_torus_cells(Box b, Tabs T, TorusK m, double* prim, double* eps) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.count()) return;
+    const int j = (int)(t % b.SX) - 2, k = (int)((t / b.SX) % b.SY) - 2, l = (int)(t / ((long long)b.SX * b.SY)) - 2;
+    double v[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, e = 0.0;
+    if (j >= 1 && j <= b.nx && k >= 1 && k <= b.ny && l >= 1 && l <= b.nz)
+        torus_cell(T, m, j, k, v[IRHO], v[IVZ], v[ITAU], e);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) prim[8 * t + q] = v[q];
+    eps[t] = e;
+}
+
+// A_phi = max(rho - rho_cut, 0)/rho_max on the active cells (zero elsewhere),
+// averaged over (j, j+1) x (l, l+1) at the corner (model.f90:126-146)
+__device__ __forceinline__ double torus_corner(const Box& b, const TorusK& m, const double* prim, int j, int k, int l) {
+    if (j < 1 || j > b.nx || k < 1 || k > b.ny || l < 1 || l > b.nz) return 0.0;
+    auto A = [&](int jj, int ll) -> double {
+        if (jj > b.nx || ll > b.nz) return 0.0;
+        const double rho = prim[8LL * b.idx(jj, k, ll) + IRHO];
+        return rho >= m.rho_cut ? (rho - m.rho_cut) / m.rho_max : 0.0;
+    };
+    return 0.25 * (((A(j, l) + A(j + 1, l)) + A(j, l + 1)) + A(j + 1, l + 1));
+}
+
+// face fields on 0:n (model.f90:153-162): B = curl(A_phi)
+__global__ void __launch_bounds__(256) k_torus_faces(Box b, Tabs T, TorusK m, double* prim) {
+    const long long n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n0 * n1 * n2) return;
+    const int j = (int)(t % n0), k = (int)((t / n0) % n1), l = (int)(t / (n0 * n1));
+    const double a = torus_corner(b, m, prim, j, k, l);
+    const double akm = torus_corner(b, m, prim, j, k - 1, l);
+    const double ajm = torus_corner(b, m, prim, j - 1, k, l);
+    const double xfj = T.ax[0].f[j], xfjm = T.ax[0].f[j - 1];
+    const long long i = b.idx(j, k, l);
+    prim[8 * i + IBX] = (T.sinf[k] * a - T.sinf[k - 1] * akm) / (xfj * T.dcos[k]);
+    prim[8 * i + IBY] = -(xfj * a - xfjm * ajm) / (T.ax[0].c[j] * T.ax[0].d[j]);
+}
+
+// maxima of p and of the cell magnetic pressure over the active cells
+// (model.f90:176-219), as 64-bit patterns of non-negative doubles
+__global__ void __launch_bounds__(256) k_torus_max(Box b, const double* prim, unsigned long long* mx) {
+    const long long total = (long long)b.nx * b.ny * b.nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double pg = 0.0, pm = 0.0;
+    if (t < total) {
+        const int j = (int)(t % b.nx) + 1, k = (int)((t / b.nx) % b.ny) + 1, l = (int)(t / ((long long)b.nx * b.ny)) + 1;
+        const long long i = b.idx(j, k, l);
+        const double bcx = 0.5 * (prim[8 * i + IBX] + prim[8LL * b.idx(j - 1, k, l) + IBX]);
+        const double bcy = 0.5 * (prim[8 * i + IBY] + prim[8LL * b.idx(j, k - 1, l) + IBY]);
+        pg = prim[8 * i + ITAU];
+        pm = 0.5 * (bcx * bcx + bcy * bcy);
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        pg = fmax(pg, __shfl_xor_sync(0xffffffffu, pg, s));
+        pm = fmax(pm, __shfl_xor_sync(0xffffffffu, pm, s));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(mx, (unsigned long long)__double_as_longlong(pg));
+        atomicMax(mx + 1, (unsigned long long)__double_as_longlong(pm));
+    }
+}
+
+// normalise the face fields to plasma beta, then the seeded density noise
+// (model.f90:256-265): rho (1 + noise (2u - 1)) where rho > rho_floor
+__global__ void __launch_bounds__(256) k_torus_finish(Box b, TorusK m, const unsigned long long* mx, double* prim) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= b.count()) return;
+    const int j = (int)(t % b.SX) - 2, k = (int)((t / b.SX) % b.SY) - 2, l = (int)(t / ((long long)b.SX * b.SY)) - 2;
+    if (j >= 0 && j <= b.nx && k >= 0 && k <= b.ny && l >= 0 && l <= b.nz) {
+        const double pg = __longlong_as_double((long long)mx[0]), pm = __longlong_as_double((long long)mx[1]);
+        const double norm = pm > 0.0 ? sqrt((pg / pm) / m.beta) : 0.0;
+        prim[8 * t + IBX] *= norm;
+        prim[8 * t + IBY] *= norm;
+    }
+    if (j >= 1 && j <= b.nx && k >= 1 && k <= b.ny && l >= 1 && l <= b.nz) {
+        const unsigned long long idx =
+            (unsigned long long)(j - 1) + (unsigned long long)b.nx * ((unsigned long long)(k - 1) + (unsigned long long)b.ny * (l - 1));
+        // splitmix64(seed, idx) -> [0, 1) with 53 bits (problems.uniform01)
+        unsigned long long z = m.seed * 0xD1B54A32D192ED03ULL + (idx + 1ULL) * 0x9E3779B97F4A7C15ULL;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        z = z ^ (z >> 31);
+        const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+        const double d = prim[8 * t + IRHO];
+        if (d > m.rho_floor) prim[8 * t + IRHO] = d + d * (u - 0.5) / 0.5 * m.noise;
+    }
 }
 
 // halo planes of a z face: the 11 arrays a neighbouring slab reads in its
@@ -1536,5 +1654,55 @@ extern "C" int cumc_restore_state(cumc_ctx* c, const double* host_state) {
     c->ready = true;
     c->next_stage = 1;
     c->bf_set = c->cur;
+    return sync_status(c);
+}
+
+// ---------------------------------------------------------------------------
+// cumc_model_torus: GET_MODEL of the spherical torus on the device
+// ---------------------------------------------------------------------------
+extern "C" int cumc_model_torus(cumc_ctx* c, const cumc_torus_model* p) {
+    if (!c || !p) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
+    if (c->coord != CUMC_SPHERICAL) return c->fail(CUMC_ERR_CONFIG, "the torus model needs CUMC_SPHERICAL");
+    const double g = c->ggas, q = p->q_grad, rsh = p->r_sh;
+    auto schw = [&](double r) { return -1.0 / (r - rsh); };
+    TorusK m;
+    m.ggas = g;
+    m.r_sh = rsh;
+    m.s_in = p->s_in;
+    m.q = q;
+    m.lkep2 = std::pow(p->s_max, 2.0 * q - 1.0) / std::pow(p->s_max - rsh, 2.0);
+    m.c_const = schw(p->s_in) - m.lkep2 * std::pow(p->s_in, 2.0 - 2.0 * q) / (2.0 - 2.0 * q);
+    const double h_max = -schw(p->s_max) + m.lkep2 * std::pow(p->s_max, 2.0 - 2.0 * q) / (2.0 - 2.0 * q) + m.c_const;
+    m.k_poly = h_max * (g - 1.0) / g / std::pow(p->rho_max, g - 1.0);
+    if (!(m.k_poly >= 0.0)) return c->fail(CUMC_ERR_CONFIG, "the polytropic constant is negative");
+    m.rho_a = p->rho_fac * p->rho_max;
+    m.rho_max = p->rho_max;
+    m.rho_cut = p->rho_cut;
+    m.beta = p->beta;
+    m.noise = p->noise;
+    m.rho_floor = p->rho_fac * p->rho_max;
+    m.seed = p->seed;
+    int rc = ensure_staging(c);
+    if (rc != CUMC_OK) return rc;
+    if (!c->model_max && (rc = dalloc(c, &c->model_max, 2)) != CUMC_OK) return rc;
+    const Box& b = c->box;
+    const size_t NT = (size_t)b.count();
+    double* prim = c->staging;
+    double* eps = c->staging + 8 * NT;
+    launch(c, -1, (long long)NT, 256, k_torus_cells, b, c->tabs, m, prim, eps);
+    launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_torus_faces, b, c->tabs, m, prim);
+    CUMC_CHECK(cudaMemsetAsync(c->model_max, 0, 2 * sizeof(unsigned long long), c->stream));
+    launch(c, -1, (long long)b.nx * b.ny * b.nz, 256, k_torus_max, b, (const double*)prim, c->model_max);
+    launch(c, -1, (long long)NT, 256, k_torus_finish, b, m, (const unsigned long long*)c->model_max, prim);
+    if (!c->mixed) {  // the FP64 state arrays, as cumc_upload_state fills them
+        double* dst[9] = {c->w[0], c->w[1], c->w[2], c->w[3], c->w[4],
+                          c->U[c->cur][IBX], c->U[c->cur][IBY], c->U[c->cur][IBZ], c->eps};
+        CUMC_CHECK(cudaMemcpyAsync(c->dsoa, dst, 8 * sizeof(double*), cudaMemcpyHostToDevice, c->stream));
+        launch(c, -1, (long long)NT, 256, k_aos_to_soa, (long long)NT, 8, (const double*)prim, c->dsoa);
+        CUMC_CHECK(cudaMemcpyAsync(c->eps, eps, NT * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    }
+    CUMC_CHECK(cudaStreamSynchronize(c->stream));
+    c->uploaded = true;
+    c->ready = false;
     return sync_status(c);
 }

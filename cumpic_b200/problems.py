@@ -48,6 +48,7 @@ class Problem:
     r_sh: float = 0.0
     geom_source_repeat: int = 8
     precision: int = N.FP64
+    model_params: dict | None = None  # device-side generator parameters (cumc_model_torus)
 
     def config(self) -> N.CumcConfig:
         """Fill a cumc_config; the face arrays stay owned by this object."""
@@ -269,13 +270,17 @@ def shell(coordinate: int, nx: int = 16, ny: int = 12, nz: int = 10, ggas: float
 def torus(nr: int = 192, nth: int = 128, nph: int = 64, ggas: float = 5.0 / 3.0, cfl: float = 0.4,
           r_in: float = 2.0, r_out: float = 50.0, s_in: float = 6.0, s_max: float = 10.0, q_grad: float = 2.0,
           rho_max: float = 1.0, rho_fac: float = 1.0e-5, rho_cut: float = 0.2, beta: float = 100.0,
-          noise: float = 0.01, seed: int = 2, geom_source_repeat: int = 8) -> Problem:
+          noise: float = 0.01, seed: int = 2, geom_source_repeat: int = 8, host_arrays: bool = True) -> Problem:
     """Magnetised constant-angular-momentum torus on a spherical-polar grid,
     following model/torus_sph/src/model.f90:8-284 with a point-mass potential
     (r_sh = 0), log-spaced radial faces r_f(j) = r_in (r_out/r_in)^(j/nr) (the
     CUSTOM_GRID hook, solver/coords.f90:37), A_phi = max(rho - rho_cut, 0)
     (model/torus_cyn/src/model.f90:126, zero elsewhere) normalised to
-    p_gas,max / p_mag,max = beta, and seeded density noise rho*(1 + noise(2u-1))."""
+    p_gas,max / p_mag,max = beta, and seeded density noise rho*(1 + noise(2u-1)).
+    With host_arrays=False only the grid and configuration are built (prim
+    and eps are None): the state then comes from the device-side generator
+    (CUMC3D.generate_model, cumc_model_torus), which builds the same torus on
+    the GPU."""
     r_sh = 0.0
     xf = np.array([r_in * (r_out / r_in) ** (j / nr) for j in range(-3, nr + 4)], dtype=np.float64)
     yf = uniform_faces(0.05 * math.pi, 0.95 * math.pi, nth)
@@ -285,12 +290,20 @@ def torus(nr: int = 192, nth: int = 128, nph: int = 64, ggas: float = 5.0 / 3.0,
     def schw(r):
         return -1.0 / (r - r_sh)
 
+    params = dict(r_sh=r_sh, s_in=s_in, s_max=s_max, q_grad=q_grad, rho_max=rho_max, rho_fac=rho_fac,
+                  rho_cut=rho_cut, beta=beta, noise=noise, seed=seed)
     lkep2 = s_max ** (2.0 * q_grad - 1.0) / (s_max - r_sh) ** 2
     c_const = schw(s_in) - lkep2 * s_in ** (2.0 - 2.0 * q_grad) / (2.0 - 2.0 * q_grad)
     h_max = -schw(s_max) + lkep2 * s_max ** (2.0 - 2.0 * q_grad) / (2.0 - 2.0 * q_grad) + c_const
     k_poly = h_max * (ggas - 1.0) / ggas / rho_max ** (ggas - 1.0)
     if k_poly < 0.0:
         raise ValueError("the polytropic constant is negative")
+    rho_floor = rho_fac * rho_max
+    eps_floor = k_poly * rho_floor ** (ggas - 1.0) / (ggas - 1.0)
+    if not host_arrays:
+        return Problem(f"torus_{nr}x{nth}x{nph}", nr, nth, nph, xf, yf, zf, N.SPHERICAL, (1, 1, 3, 3, 0, 0), ggas,
+                       cfl, 0.0, None, None, model=N.MODEL_TORUS_SPH, rho_floor=rho_floor, eps_floor=eps_floor,
+                       r_sh=r_sh, geom_source_repeat=geom_source_repeat, model_params=params)
     rc = _centres(xf)   # index i+2 -> cell i
     tc = _centres(yf)
     r = rc[3:nr + 3][None, None, :]
@@ -344,8 +357,6 @@ def torus(nr: int = 192, nth: int = 128, nph: int = 64, ggas: float = 5.0 / 3.0,
     norm = math.sqrt((pgas_max / pmag_max) / beta) if pmag_max > 0 else 0.0
     prim[sl0 + (IBX,)] *= norm
     prim[sl0 + (IBY,)] *= norm
-    rho_floor = rho_fac * rho_max
-    eps_floor = k_poly * rho_floor ** (ggas - 1.0) / (ggas - 1.0)
     # density noise where rho > rho_floor (model.f90:256-265, seeded)
     idx = _linear_index(nr, nth, nph)[1:, 1:, 1:]
     u = uniform01(seed, idx)
@@ -353,4 +364,4 @@ def torus(nr: int = 192, nth: int = 128, nph: int = 64, ggas: float = 5.0 / 3.0,
     prim[sl1 + (IRHO,)] = np.where(d > rho_floor, d + d * (u - 0.5) / 0.5 * noise, d)
     return Problem(f"torus_{nr}x{nth}x{nph}", nr, nth, nph, xf, yf, zf, N.SPHERICAL, (1, 1, 3, 3, 0, 0), ggas,
                    cfl, 0.0, prim, eps, model=N.MODEL_TORUS_SPH, rho_floor=rho_floor, eps_floor=eps_floor,
-                   r_sh=r_sh, geom_source_repeat=geom_source_repeat)
+                   r_sh=r_sh, geom_source_repeat=geom_source_repeat, model_params=params)

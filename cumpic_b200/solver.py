@@ -67,6 +67,15 @@ class CUMC3D:
         eps = np.ascontiguousarray(self.problem.eps if eps is None else eps, dtype=np.float64)
         self._check(self._lib.cumc_upload_state(self._h, _dp(prim), _dp(eps)))
 
+    def generate_model(self):
+        """the initial state built on the device (cumc_model_torus) from the
+        problem's model_params, in place of upload"""
+        mp = self.problem.model_params
+        if not mp:
+            raise ValueError("the problem has no device-side generator parameters")
+        m = N.CumcTorusModel(**mp)
+        self._check(self._lib.cumc_model_torus(self._h, ctypes.byref(m)))
+
     def initial_update(self):
         """initial_update (solver/initial.f90:83-140)."""
         self._check(self._lib.cumc_initial_update(self._h))

@@ -177,6 +177,25 @@ int cumc_profile_read(cumc_ctx* ctx, int which, int* launches, double* ms);
 /* Number of kernel launches the library issued since cumc_init. */
 int cumc_launch_count(cumc_ctx* ctx, long long* count);
 
+/* Device-side GET_MODEL of the spherical torus (model/torus_sph/src/
+ * model.f90:8-284), for grids too large to build on the host: a
+ * constant-angular-momentum torus around a point mass at r_sh (potential
+ * -1/(r - r_sh)), polytropic with p = K rho^gamma, density floor
+ * rho_fac * rho_max outside; A_phi = max(rho - rho_cut, 0)/rho_max on the
+ * cells, averaged to the corners, face fields B = curl A normalised to
+ * max p_gas / max p_mag = beta; then density noise rho (1 + noise (2u - 1))
+ * where rho > rho_fac * rho_max, u from splitmix64(seed, linear cell index).
+ * Fills the state as cumc_upload_state would (call cumc_initial_update
+ * next); the grid is the context's (CUMC_SPHERICAL, else CUMC_ERR_CONFIG).
+ * The host generator cumpic_b200.problems.torus builds the same state. */
+typedef struct {
+    double r_sh, s_in, s_max, q_grad;   /* potential centre, torus inner edge, pressure maximum, l ~ s^(2-q) */
+    double rho_max, rho_fac, rho_cut;   /* peak density, floor factor, field threshold */
+    double beta, noise;                 /* plasma beta of the maxima, density noise amplitude */
+    unsigned long long seed;
+} cumc_torus_model;
+int cumc_model_torus(cumc_ctx* ctx, const cumc_torus_model* model);
+
 /* z-slab decomposition: the halo exchange between slabs (replaces the MPI
  * path of solver/mpi.f90:255-501, MPI_BOUNDARYP_Z / MPI_BOUNDARY_Z, and the
  * internal faces of solver/boundary.f90:332-336,663-667). A z face whose
