@@ -365,3 +365,83 @@ def torus(nr: int = 192, nth: int = 128, nph: int = 64, ggas: float = 5.0 / 3.0,
     return Problem(f"torus_{nr}x{nth}x{nph}", nr, nth, nph, xf, yf, zf, N.SPHERICAL, (1, 1, 3, 3, 0, 0), ggas,
                    cfl, 0.0, prim, eps, model=N.MODEL_TORUS_SPH, rho_floor=rho_floor, eps_floor=eps_floor,
                    r_sh=r_sh, geom_source_repeat=geom_source_repeat, model_params=params)
+
+
+def torus_cyl(nr: int = 32, nph: int = 8, nz: int = 32, ggas: float = 5.0 / 3.0, cfl: float = 0.4,
+              r_in: float = 1.5, r_out: float = 8.0, z_half: float = 3.0, r_sh: float = 1.0, s_in: float = 3.0,
+              s_max: float = 4.7, q_grad: float = 2.0, rho_max: float = 1.0, rho_fac: float = 1.0e-4,
+              rho_cut: float = 0.5, beta: float = 100.0, noise: float = 1.0e-4, seed: int = 4,
+              geom_source_repeat: int = 8) -> Problem:
+    """Magnetised torus on a cylindrical grid (R, phi, z), following
+    model/torus_cyn/src/model.f90:8-284: the pseudo-Newtonian potential
+    -1/(sqrt(R^2 + z^2) - r_sh), angular momentum l^2 ~ R^(2-2q) from the
+    Keplerian value at s_max, polytropic p = K rho^gamma with the torus
+    inside R >= s_in and the floor rho_fac*rho_max outside; v_phi = sqrt(l_kep^2)
+    R^(1-q); A_phi = max(rho - rho_cut, 0)/rho_max on the cells, averaged over
+    (R, z) to the corners, B_R = -dA/dz and B_z = (1/R) d(R A)/dR on the faces,
+    normalised to p_gas,max / p_mag,max = beta (the cell B_z of that ratio
+    averages over the phi neighbour, as model.f90:166 does); then seeded
+    density noise rho (1 + noise (2u - 1)) where rho > rho_floor. Faces:
+    outflow in R and z (the model's ghost clamps apply there), periodic in phi."""
+    xf = uniform_faces(r_in, r_out, nr)
+    yf = uniform_faces(0.0, 2.0 * math.pi, nph)
+    zf = uniform_faces(-z_half, z_half, nz)
+    prim, eps = _empty(nr, nph, nz)
+
+    def schw(r, z):
+        return -1.0 / (np.sqrt(r ** 2 + z ** 2) - r_sh)
+
+    lkep2 = s_max ** (2.0 * q_grad - 1.0) / (s_max - r_sh) ** 2
+    c_const = float(schw(s_in, 0.0)) - lkep2 * s_in ** (2.0 - 2.0 * q_grad) / (2.0 - 2.0 * q_grad)
+    h_max = -float(schw(s_max, 0.0)) + lkep2 * s_max ** (2.0 - 2.0 * q_grad) / (2.0 - 2.0 * q_grad) + c_const
+    k_poly = h_max * (ggas - 1.0) / ggas / rho_max ** (ggas - 1.0)
+    if k_poly < 0.0:
+        raise ValueError("the polytropic constant is negative")
+    R = _centres(xf)[3:nr + 3][None, None, :]
+    Z = _centres(zf)[3:nz + 3][:, None, None]
+    h = -schw(R, Z) + lkep2 * R ** (2.0 - 2.0 * q_grad) / (2.0 - 2.0 * q_grad) + c_const
+    h = np.maximum(h, 0.0)
+    rho_loc = (h * (ggas - 1.0) / ggas / k_poly) ** (1.0 / (ggas - 1.0))
+    rho_a = rho_fac * rho_max
+    inside = (rho_loc > rho_a) & (R >= s_in)
+    rho = np.where(inside, rho_loc, rho_a) * np.ones((1, nph, 1))
+    vph = np.where(inside, np.sqrt(lkep2) * R ** (-q_grad) * R, 0.0) * np.ones((1, nph, 1))
+    sl1 = (slice(3, nz + 3), slice(3, nph + 3), slice(3, nr + 3))
+    v = prim[sl1]
+    v[..., IRHO] = rho
+    v[..., IVY] = vph
+    v[..., ITAU] = k_poly * rho ** ggas
+    eps[sl1] = k_poly * rho ** (ggas - 1.0) / (ggas - 1.0)
+    A = np.zeros((nz + 6, nph + 6, nr + 6))
+    A[sl1] = np.where(rho >= rho_cut, (rho - rho_cut) / rho_max, 0.0)
+    Ac = np.zeros_like(A)
+    Ac[sl1] = 0.25 * (A[3:nz + 3, 3:nph + 3, 3:nr + 3] + A[3:nz + 3, 3:nph + 3, 4:nr + 4]
+                      + A[4:nz + 4, 3:nph + 3, 3:nr + 3] + A[4:nz + 4, 3:nph + 3, 4:nr + 4])
+    # faces on 0:n (model.f90:149-158)
+    f0 = (slice(2, nz + 3), slice(2, nph + 3), slice(2, nr + 3))
+    a = Ac[f0]
+    a_lm = Ac[1:nz + 2, 2:nph + 3, 2:nr + 3]    # (j, k, l-1)
+    a_jm = Ac[2:nz + 3, 2:nph + 3, 1:nr + 2]    # (j-1, k, l)
+    xfj = xf[3:nr + 4][None, None, :]           # faces j = 0..n
+    xfjm = xf[2:nr + 3][None, None, :]
+    xl = 0.5 * (xfj + xfjm)
+    dxl = xfj - xfjm
+    dzl = (zf[3:nz + 4] - zf[2:nz + 3])[:, None, None]
+    prim[f0 + (IBX,)] = -(a - a_lm) / dzl
+    prim[f0 + (IBZ,)] = (xfj * a - xfjm * a_jm) / (xl * dxl)
+    # beta normalisation (model.f90:162-214)
+    bcx = 0.5 * (prim[sl1 + (IBX,)] + prim[3:nz + 3, 3:nph + 3, 2:nr + 2, IBX])
+    bcz = 0.5 * (prim[sl1 + (IBZ,)] + prim[3:nz + 3, 2:nph + 2, 3:nr + 3, IBZ])
+    pgas_max = prim[sl1 + (ITAU,)].max()
+    pmag_max = (0.5 * (bcx ** 2 + bcz ** 2)).max()
+    norm = math.sqrt((pgas_max / pmag_max) / beta) if pmag_max > 0 else 0.0
+    prim[f0 + (IBX,)] *= norm
+    prim[f0 + (IBZ,)] *= norm
+    rho_floor = rho_fac * rho_max
+    eps_floor = k_poly * rho_floor ** (ggas - 1.0) / (ggas - 1.0)
+    u = uniform01(seed, _linear_index(nr, nph, nz)[1:, 1:, 1:])
+    d = prim[sl1 + (IRHO,)]
+    prim[sl1 + (IRHO,)] = np.where(d > rho_floor, d + d * (u - 0.5) / 0.5 * noise, d)
+    return Problem(f"torus_cyl_{nr}x{nph}x{nz}", nr, nph, nz, xf, yf, zf, N.CYLINDRICAL, (1, 1, 0, 0, 1, 1), ggas,
+                   cfl, 0.0, prim, eps, model=N.MODEL_TORUS_CYN, rho_floor=rho_floor, eps_floor=eps_floor,
+                   r_sh=r_sh, geom_source_repeat=geom_source_repeat)

@@ -74,13 +74,15 @@ def test_mixed_advance_equals_host_loop():
     assert np.array_equal(x.download()["cons"], y.download()["cons"])
 
 
-@pytest.mark.parametrize("coord", [N.CYLINDRICAL, N.SPHERICAL])
-def test_curvilinear_shell_mixed_vs_fp64(coord):
-    """geometric flux, CT and source terms of the mixed path on the smooth
-    shells, with the FP64 run's dt sequence replayed"""
-    a = _run(P.shell(coord, 24, 20, 16), N.FP64, steps=0)
+@pytest.mark.parametrize("make", [lambda: P.shell(N.CYLINDRICAL, 24, 20, 16), lambda: P.shell(N.SPHERICAL, 24, 20, 16),
+                                  lambda: P.torus_cyl(40, 8, 40)], ids=["cyl_shell", "sph_shell", "torus_cyl"])
+def test_curvilinear_mixed_vs_fp64(make):
+    """geometric flux, CT and source terms (and the cylindrical torus's
+    gravity, floors and ghost clamps) of the mixed path, with the FP64 run's
+    dt sequence replayed"""
+    a = _run(make(), N.FP64, steps=0)
     dts = [a.step() for _ in range(10)]
-    b = _run(P.shell(coord, 24, 20, 16), N.MIXED, steps=0)
+    b = _run(make(), N.MIXED, steps=0)
     for dt in dts:
         b.rungekutta(dt)
     db = b.download()

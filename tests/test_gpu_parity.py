@@ -45,6 +45,7 @@ SMALL = [
     ("torus_small", lambda: P.torus(24, 16, 8)),
     ("torus_small_q1_once", lambda: P.torus(20, 12, 6, geom_source_repeat=1)),
     ("cylindrical_shell", lambda: P.shell(N.CYLINDRICAL, 16, 12, 10)),
+    ("torus_cylindrical", lambda: P.torus_cyl(24, 6, 20)),
     ("spherical_shell", lambda: P.shell(N.SPHERICAL, 14, 12, 10)),
 ]
 
