@@ -87,6 +87,7 @@ struct cumc_ctx {
     void* adj_slab = nullptr;       // adjoint scratch, kept between runs
     size_t adj_slab_bytes = 0;
     int next_stage = 1;    // cumc_rk_stage: the stage due next
+    bool fuse_dt = false;  // cumc_advance: stage 3 also forms the next step's CFL dt
     int bf_set = 0;        // U[bf_set] holds the current face fields (the last stage's output)
     bool exchange = false;  // a z face is CUMC_BC_EXCHANGE
     unsigned long long* model_max = nullptr;  // cumc_model_torus: the two maxima
@@ -443,7 +444,11 @@ void run_stage(cumc_ctx* c, const Box& b, int stage) {
     // Nothing reads the hydro cons outside (0:n)^3, nor a face field outside
     // 0:n along its own axis, and the boundary refills the tangential ones.
     for (int q = 0; q < 8; ++q) a.tape[q] = (c->tape && stage > 0) ? c->tape[(stage - 1) * 8 + q] : nullptr;
-    const UtopArgs o = utop_args(c, dst, PrimBufs{c->w, c->bc, c->eps});
+    UtopArgs o = utop_args(c, dst, PrimBufs{c->w, c->bc, c->eps});
+    if (stage == 3 && c->fuse_dt) {  // the following iteration's finddt, fused (dtmin reset by the caller)
+        o.dtmin = c->dtmin;
+        o.cfl = c->cfl;
+    }
     switch (c->coord) {
         case CUMC_CARTESIAN: combine_model<1>(c, b, stage, pr, ff, a, o); break;
         case CUMC_CYLINDRICAL: combine_model<2>(c, b, stage, pr, ff, a, o); break;
@@ -485,14 +490,23 @@ Clock make_clock(cumc_ctx* c) {
 }
 
 // one main-loop iteration with device-resident dt (solver/main.f90:127-143)
+// One iteration of the main loop (solver/main.f90:130-142). In the FP64
+// form dt comes from the previous iteration's stage 3 (fused finddt; the
+// caller runs a standalone finddt before the first iteration), so a step
+// reads the state once less.
 void loop_step(cumc_ctx* c, double t_end) {
     Box b = c->box;
     const Clock k = make_clock(c);
     launch(c, -1, 1, 1, k_check_done, k, t_end);
     b.skip = k.done;
-    finddt_launch(c, b);
+    if (c->mixed) finddt_launch(c, b);
     launch(c, -1, 1, 1, k_clip_dt, k, t_end);
+    if (!c->mixed) {
+        launch(c, -1, 1, 1, k_reset_dtmin, c->dtmin);
+        c->fuse_dt = true;
+    }
     rk_step(c, b);
+    c->fuse_dt = false;
     launch(c, -1, 1, 1, k_advance_time, k);
 }
 
@@ -1125,6 +1139,7 @@ int cumc_advance(cumc_ctx* c, int nsteps, double t_end, double* t_inout, int* st
     if (nsteps < 0 || !t_inout) return c->fail(CUMC_ERR_ARG, "nsteps must be >= 0 and t_inout non-null");
     launch(c, -1, 1, 1, k_set_scalar, c->scal + 1, *t_inout);
     CUMC_CHECK(cudaMemsetAsync(c->ints, 0, 2 * sizeof(int), c->stream));
+    if (nsteps > 0 && !c->mixed) finddt_launch(c, c->box);  // dt of the first iteration; stage 3 gives the rest
     if (nsteps > 0 && !c->prof_on) {
         if (!c->graph_exec || c->graph_t_end != t_end) {
             if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }

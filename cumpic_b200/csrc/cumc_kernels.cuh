@@ -156,6 +156,52 @@ __global__ void __launch_bounds__(256) k_emf(Box b, PrimT<R> pr, FaceFluxT<R> fx
     out.e[2][i] = ez;
 }
 
+// CFL step of one interior cell (solver/rungekutta.f90:201-250): the fast
+// magnetosonic speed along each axis from the cell's primitives and bcell
+template <int COORD>
+__device__ __forceinline__ double cell_dt(const Tabs& T, int j, int k, int l, double rho, double p, double vx,
+                                          double vy, double vz, double bcx, double bcy, double bcz, double ggas,
+                                          double cfl) {
+    const double cs = sqrt((ggas * p) / rho);
+    const double a2 = cs * cs;
+    const double a4 = a2 * a2;
+    const double b2x = (bcx * bcx) / rho;
+    const double b2y = (bcy * bcy) / rho;
+    const double b2z = (bcz * bcz) / rho;
+    const double b2 = (b2x + b2y) + b2z;
+    const double b4 = b2 * b2;
+    const double base = (a4 + (2.0 * a2) * b2) + b4;
+    const double cfx = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2x)));
+    const double cfy = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2y)));
+    const double cfz = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2z)));
+    const double lambda = fmax(fmax(fabs(vx) + cfx, fabs(vy) + cfy), fabs(vz) + cfz);
+    double dxl = T.ax[0].d[j], dyl = T.ax[1].d[k], dzl = T.ax[2].d[l];
+    if (COORD == 2) {
+        dyl = T.ax[0].c[j] * dyl;
+    } else if (COORD == 3) {
+        dyl = T.ax[0].c[j] * dyl;
+        dzl = (T.ax[0].c[j] * T.sinc[k]) * dzl;
+    }
+    return (fmin(fmin(dxl, dyl), dzl) * cfl) / lambda;
+}
+
+// block minimum of dt (every thread of the block calls it), then one 64-bit
+// atomicMin on the non-negative bit pattern; fmin drops NaN, as MIN does for
+// the reference's non-NaN path
+__device__ __forceinline__ void block_min_dt(double dt, unsigned long long* dtmin) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dt;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 1.0e10;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0 && v >= 0.0) atomicMin(dtmin, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
 // ----------------------------------------------------------------------------
 // The RK stage combine on (0:n)^3 (solver/rungekutta.f90:41-51,75-85,109-119).
 // Hydro l_rk (interior only) is the x, y, z flux differences in that order
@@ -336,6 +382,8 @@ struct UtopArgs {
     double* eps;
     double ggas, rho_floor, eps_floor;
     unsigned int* flag;  // bit 0: non-finite value seen
+    unsigned long long* dtmin = nullptr;  // k_combine_utop, stage 3: the next step's CFL dt (finddt fused)
+    double cfl = 0.0;
 };
 
 // bcell of cell i: the face-field average on the interior (solver/fromrvetou.f90
@@ -359,7 +407,7 @@ __device__ __forceinline__ void bcell_point(const Box& b, const UtopArgs& a, int
 // the conversions of one cell; with FROM_CONS the hydro cons come in uh
 template <int MODEL, bool FROM_CONS>
 __device__ __forceinline__ void utop_point(const UtopArgs& a, int i, bool interior, const double* uh, double bx,
-                                           double by, double bz) {
+                                           double by, double bz, double* prim_out = nullptr) {
     const double bsquare = (bx * bx + by * by) + bz * bz;
     double rho, vx, vy, vz, e;
     if (FROM_CONS) {
@@ -399,6 +447,13 @@ __device__ __forceinline__ void utop_point(const UtopArgs& a, int i, bool interi
         const double p = (rho * e) * (a.ggas - 1.0);  // EOS_PRESSURE
         a.w[4][i] = p;
         if (!(isfinite(p) && isfinite(vsquare) && isfinite(rho))) atomicOr(a.flag, 1u);
+        if (prim_out) {
+            prim_out[0] = rho;
+            prim_out[1] = vx;
+            prim_out[2] = vy;
+            prim_out[3] = vz;
+            prim_out[4] = p;
+        }
     }
 }
 
@@ -420,24 +475,38 @@ __global__ void __launch_bounds__(256) k_utop(Box b, UtopArgs a) {
 // hydro part of RK stage STAGE and the conversions, after k_ct of the same
 // stage. o.u is a.ud; w, bc and eps of o are the arrays pr reads, each at the
 // thread's own index only, before the thread writes them.
+// At stage 3, when o.dtmin is set, the kernel also forms the next step's CFL
+// dt from the primitives it has just made (the finddt of the following main-
+// loop iteration, solver/main.f90:130, fused): every thread then stays to
+// the block's min reduction.
 template <int COORD, int MODEL, int STAGE>
 __global__ void __launch_bounds__(256, 8) k_combine_utop(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy, FaceFlux fz,
                                                       CombineArgs a, UtopArgs o) {
+    if (b.skip && *b.skip) return;
     int j, k, l, i;
-    if (!box1_index(b, j, k, l, i)) return;
-    double L[5];
-    hydro_lrk<COORD, MODEL>(T, pr, fx, fy, fz, a, j, k, l, i, b.SX, b.SX * b.SY, L);
-    const double dt = *a.dt;
-    double uh[5];
+    const bool live = box1_index(b, j, k, l, i);
+    const bool fuse_dt = STAGE == 3 && o.dtmin;
+    if (!live && !fuse_dt) return;
+    double dt_cell = 1.0e10;
+    if (live) {
+        double L[5];
+        hydro_lrk<COORD, MODEL>(T, pr, fx, fy, fz, a, j, k, l, i, b.SX, b.SX * b.SY, L);
+        const double dt = *a.dt;
+        double uh[5];
 #pragma unroll
-    for (int q = 0; q < 5; ++q) {
-        uh[q] = rk_point<STAGE>(a.u0[q][i], STAGE == 1 ? 0.0 : a.uc[q][i], dt, L[q]);
-        if (a.tape[q]) a.tape[q][i] = uh[q];
+        for (int q = 0; q < 5; ++q) {
+            uh[q] = rk_point<STAGE>(a.u0[q][i], STAGE == 1 ? 0.0 : a.uc[q][i], dt, L[q]);
+            if (a.tape[q]) a.tape[q][i] = uh[q];
+        }
+        const bool interior = j >= 1 && k >= 1 && l >= 1;
+        double bx, by, bz;
+        bcell_point(b, o, i, interior, bx, by, bz);
+        double pw[5];
+        utop_point<MODEL, true>(o, i, interior, uh, bx, by, bz, fuse_dt ? pw : nullptr);
+        if (fuse_dt && interior)
+            dt_cell = cell_dt<COORD>(T, j, k, l, pw[0], pw[4], pw[1], pw[2], pw[3], bx, by, bz, o.ggas, o.cfl);
     }
-    const bool interior = j >= 1 && k >= 1 && l >= 1;
-    double bx, by, bz;
-    bcell_point(b, o, i, interior, bx, by, bz);
-    utop_point<MODEL, true>(o, i, interior, uh, bx, by, bz);
+    if (fuse_dt) block_min_dt(dt_cell, o.dtmin);
 }
 
 // ----------------------------------------------------------------------------
@@ -608,43 +677,10 @@ __global__ void __launch_bounds__(256) k_finddt(Box b, Tabs T, PrimT<R> pr, doub
         const int k = (int)((t / b.nx) % b.ny) + 1;
         const int l = (int)(t / ((long long)b.nx * b.ny)) + 1;
         const int i = b.idx(j, k, l);
-        const double rho = pr.w[0][i];
-        const double cs = sqrt((ggas * (double)pr.w[4][i]) / rho);
-        const double a2 = cs * cs;
-        const double a4 = a2 * a2;
-        const double bcx = pr.bc[0][i], bcy = pr.bc[1][i], bcz = pr.bc[2][i];
-        const double b2x = (bcx * bcx) / rho;
-        const double b2y = (bcy * bcy) / rho;
-        const double b2z = (bcz * bcz) / rho;
-        const double b2 = (b2x + b2y) + b2z;
-        const double b4 = b2 * b2;
-        const double base = (a4 + (2.0 * a2) * b2) + b4;
-        const double cfx = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2x)));
-        const double cfy = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2y)));
-        const double cfz = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2z)));
-        const double vx = pr.w[1][i], vy = pr.w[2][i], vz = pr.w[3][i];
-        const double lambda = fmax(fmax(fabs(vx) + cfx, fabs(vy) + cfy), fabs(vz) + cfz);
-        double dxl = T.ax[0].d[j], dyl = T.ax[1].d[k], dzl = T.ax[2].d[l];
-        if (COORD == 2) {
-            dyl = T.ax[0].c[j] * dyl;
-        } else if (COORD == 3) {
-            dyl = T.ax[0].c[j] * dyl;
-            dzl = (T.ax[0].c[j] * T.sinc[k]) * dzl;
-        }
-        dt_out = (fmin(fmin(dxl, dyl), dzl) * cfl) / lambda;
+        dt_out = cell_dt<COORD>(T, j, k, l, pr.w[0][i], (double)pr.w[4][i], pr.w[1][i], pr.w[2][i], pr.w[3][i],
+                                pr.bc[0][i], pr.bc[1][i], pr.bc[2][i], ggas, cfl);
     }
-    // fmin drops NaN, as MIN does for the reference's non-NaN path
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) dt_out = fmin(dt_out, __shfl_xor_sync(0xffffffffu, dt_out, o));
-    __shared__ double red[32];
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dt_out;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 1.0e10;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (threadIdx.x == 0 && v >= 0.0) atomicMin(dtmin, (unsigned long long)__double_as_longlong(v));
-    }
+    block_min_dt(dt_out, dtmin);
 }
 
 // ----------------------------------------------------------------------------
