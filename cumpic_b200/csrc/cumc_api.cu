@@ -410,7 +410,8 @@ Launcher mx_launcher(cumc_ctx* c) { return Launcher{c->stream, mx_pre, mx_post, 
 // stage 0: SPATIAL only, l_rk stored in c->L.
 void run_stage(cumc_ctx* c, const Box& b, int stage) {
     if (c->mixed) {
-        if (stage > 0) mixed_stage(mx_launcher(c), b, c->tabs, c->mb, c->mp, stage);
+        if (stage > 0)
+            mixed_stage(mx_launcher(c), b, c->tabs, c->mb, c->mp, stage, stage == 3 && c->fuse_dt ? c->dtmin : nullptr);
         return;
     }
     double* const* Un = c->U[c->cur];
@@ -490,21 +491,18 @@ Clock make_clock(cumc_ctx* c) {
 }
 
 // one main-loop iteration with device-resident dt (solver/main.f90:127-143)
-// One iteration of the main loop (solver/main.f90:130-142). In the FP64
-// form dt comes from the previous iteration's stage 3 (fused finddt; the
-// caller runs a standalone finddt before the first iteration), so a step
-// reads the state once less.
+// One iteration of the main loop (solver/main.f90:130-142). dt comes from
+// the previous iteration's stage 3 (fused finddt, in both forms; the caller
+// runs a standalone finddt before the first iteration), so a step reads the
+// state once less.
 void loop_step(cumc_ctx* c, double t_end) {
     Box b = c->box;
     const Clock k = make_clock(c);
     launch(c, -1, 1, 1, k_check_done, k, t_end);
     b.skip = k.done;
-    if (c->mixed) finddt_launch(c, b);
     launch(c, -1, 1, 1, k_clip_dt, k, t_end);
-    if (!c->mixed) {
-        launch(c, -1, 1, 1, k_reset_dtmin, c->dtmin);
-        c->fuse_dt = true;
-    }
+    launch(c, -1, 1, 1, k_reset_dtmin, c->dtmin);
+    c->fuse_dt = true;
     rk_step(c, b);
     c->fuse_dt = false;
     launch(c, -1, 1, 1, k_advance_time, k);
@@ -1139,7 +1137,7 @@ int cumc_advance(cumc_ctx* c, int nsteps, double t_end, double* t_inout, int* st
     if (nsteps < 0 || !t_inout) return c->fail(CUMC_ERR_ARG, "nsteps must be >= 0 and t_inout non-null");
     launch(c, -1, 1, 1, k_set_scalar, c->scal + 1, *t_inout);
     CUMC_CHECK(cudaMemsetAsync(c->ints, 0, 2 * sizeof(int), c->stream));
-    if (nsteps > 0 && !c->mixed) finddt_launch(c, c->box);  // dt of the first iteration; stage 3 gives the rest
+    if (nsteps > 0) finddt_launch(c, c->box);  // dt of the first iteration; stage 3 gives the rest
     if (nsteps > 0 && !c->prof_on) {
         if (!c->graph_exec || c->graph_t_end != t_end) {
             if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }

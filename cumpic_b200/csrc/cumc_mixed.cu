@@ -208,15 +208,18 @@ struct UtopMx {
     float* bf[3];
     double ggas, rho_floor, eps_floor;
     unsigned int* flag;
+    unsigned long long* dtmin = nullptr;  // FINAL: the next step's CFL dt (finddt fused)
+    double cfl = 0.0;
 };
 
-// FINAL: the state is U^n (after stage 3); otherwise U^n + d
-template <int MODEL, bool FINAL>
-__global__ void __launch_bounds__(256, 8) k_utop_mx(Box b, UtopMx a) {
-    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
-    const long long total = (long long)n0 * n1 * n2;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total || (b.skip && *b.skip)) return;
+// FINAL: the state is U^n (after stage 3); otherwise U^n + d. With a.dtmin
+// set (FINAL only) the kernel also forms the next step's CFL dt from the FP32
+// primitives it stores, widened as k_finddt<float> reads them; every thread
+// then stays to the block's min reduction.
+// one cell (flat index t on (0:n)^3); returns its CFL dt when fuse_dt, else 1e10
+template <int COORD, int MODEL, bool FINAL>
+__device__ __forceinline__ double utop_mx_cell(const Box& b, const Tabs& T, const UtopMx& a, long long t, bool fuse_dt) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1;
     const int j = (int)(t % n0);
     const int k = (int)((t / n0) % n1);
     const int l = (int)(t / ((long long)n0 * n1));
@@ -278,10 +281,30 @@ __global__ void __launch_bounds__(256, 8) k_utop_mx(Box b, UtopMx a) {
     a.w[1][i] = (float)vx;
     a.w[2][i] = (float)vy;
     a.w[3][i] = (float)vz;
+    double dt_cell = 1.0e10;
     if (interior) {
         a.w[4][i] = (float)p;
         if (!(isfinite(p) && isfinite(vsq) && isfinite(rn))) atomicOr(a.flag, 1u);
+        if (fuse_dt)
+            dt_cell = cell_dt<COORD>(T, j, k, l, (double)(float)rn, (double)(float)p, (double)(float)vx,
+                                     (double)(float)vy, (double)(float)vz, (double)a.bc[0][i], (double)a.bc[1][i],
+                                     (double)a.bc[2][i], a.ggas, a.cfl);
     }
+    return dt_cell;
+}
+
+// the block reduction has one call site, which every thread of the block
+// reaches (its warp shuffles and barrier need all of them)
+template <int COORD, int MODEL, bool FINAL>
+__global__ void __launch_bounds__(256, 8) k_utop_mx(Box b, Tabs T, UtopMx a) {
+    const long long total = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b.skip && *b.skip) return;  // the same for every thread
+    const bool fuse_dt = FINAL && a.dtmin;
+    if (t >= total && !fuse_dt) return;
+    double dt_cell = 1.0e10;
+    if (t < total) dt_cell = utop_mx_cell<COORD, MODEL, FINAL>(b, T, a, t, fuse_dt);
+    if (fuse_dt) block_min_dt(dt_cell, a.dtmin);
 }
 
 // initial_update from the uploaded FP64 model (AoS staging): CUSTOM_CHECKRHO,
@@ -467,7 +490,8 @@ cudaError_t mixed_attributes() {
     return cudaSuccess;
 }
 
-void mixed_stage(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p, int stage) {
+void mixed_stage(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p, int stage,
+                 unsigned long long* dtmin) {
     PrimT<float> pr;
     for (int q = 0; q < 5; ++q) pr.w[q] = m.w[q];
     for (int q = 0; q < 3; ++q) { pr.bc[q] = m.bc[q]; pr.bf[q] = m.bf[q]; }
@@ -487,17 +511,28 @@ void mixed_stage(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs
         case 2: combine_model_mx<2>(L, b, T, m, p, stage); break;
         default: combine_model_mx<3>(L, b, T, m, p, stage); break;
     }
-    const UtopMx a = utop_args(m, p);
-    const dim3 g = g1((long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256);
-#define CUMC_MX_UTOP(M)                                                       \
-    if (stage == 3) run(L, 5, g, 256, 0, k_utop_mx<M, true>, b, a);           \
-    else run(L, 5, g, 256, 0, k_utop_mx<M, false>, b, a);
-    switch (p.model) {
-        case 0: CUMC_MX_UTOP(0) break;
-        case 1: CUMC_MX_UTOP(1) break;
-        case 2: CUMC_MX_UTOP(2) break;
-        default: CUMC_MX_UTOP(3) break;
+    UtopMx a = utop_args(m, p);
+    if (stage == 3 && dtmin) {  // the following iteration's finddt, fused (dtmin reset by the caller)
+        a.dtmin = dtmin;
+        a.cfl = p.cfl;
     }
+    const dim3 g = g1((long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256);
+#define CUMC_MX_UTOP(C, M)                                                          \
+    if (stage == 3) run(L, 5, g, 256, 0, k_utop_mx<C, M, true>, b, T, a);           \
+    else run(L, 5, g, 256, 0, k_utop_mx<C, M, false>, b, T, a);
+#define CUMC_MX_UTOP_MODEL(C)                    \
+    switch (p.model) {                           \
+        case 0: CUMC_MX_UTOP(C, 0) break;        \
+        case 1: CUMC_MX_UTOP(C, 1) break;        \
+        case 2: CUMC_MX_UTOP(C, 2) break;        \
+        default: CUMC_MX_UTOP(C, 3) break;       \
+    }
+    switch (p.coord) {
+        case 1: CUMC_MX_UTOP_MODEL(1) break;
+        case 2: CUMC_MX_UTOP_MODEL(2) break;
+        default: CUMC_MX_UTOP_MODEL(3) break;
+    }
+#undef CUMC_MX_UTOP_MODEL
 #undef CUMC_MX_UTOP
     boundary_mx(L, b, m, p);
 }

@@ -50,7 +50,10 @@ struct Launcher {
 };
 
 cudaError_t mixed_attributes();
-void mixed_stage(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p, int stage);
+// stage 3 with dtmin non-null also forms the next step's CFL dt (atomicMin
+// into dtmin, which the caller has reset)
+void mixed_stage(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p, int stage,
+                 unsigned long long* dtmin = nullptr);
 void mixed_initial(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p,
                    const double* prim_aos, const double* eps_aos);
 void mixed_finddt(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs& m, const MixedParams& p,
