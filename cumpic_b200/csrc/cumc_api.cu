@@ -517,14 +517,24 @@ void loop_step(cumc_ctx* c, double t_end) {
 struct TorusK {
     double ggas, r_sh, s_in, q, lkep2, c_const, k_poly, rho_a, rho_max, rho_cut, beta, noise, rho_floor;
     unsigned long long seed;
+    int cyl;  // 1: cylindrical torus (model/torus_cyn), 0: spherical (model/torus_sph)
 };
 
-// equilibrium of cell (j, k) (active): rho, v_phi, p, eps
-__device__ __forceinline__ void torus_cell(const Tabs& T, const TorusK& m, int j, int k, double& rho, double& vph,
+// equilibrium of cell (j, k, l) (active): rho, v_phi, p, eps. Spherical:
+// potential -1/(r - r_sh), cylindrical radius s = r sin(theta);
+// cylindrical: potential -1/(sqrt(R^2 + z^2) - r_sh), s = R
+__device__ __forceinline__ void torus_cell(const Tabs& T, const TorusK& m, int j, int k, int l, double& rho, double& vph,
                                            double& p, double& eps) {
     const double r = T.ax[0].c[j];
-    const double s_eq = r * T.sinc[k];
-    const double schw = -1.0 / (r - m.r_sh);
+    double s_eq, schw;
+    if (m.cyl) {
+        const double z = T.ax[2].c[l];
+        s_eq = r;
+        schw = -1.0 / (sqrt(r * r + z * z) - m.r_sh);
+    } else {
+        s_eq = r * T.sinc[k];
+        schw = -1.0 / (r - m.r_sh);
+    }
     double h = -schw + m.lkep2 * pow(s_eq, 2.0 - 2.0 * m.q) / (2.0 - 2.0 * m.q) + m.c_const;
     h = fmax(h, 0.0);
     const double rho_loc = pow(h * (m.ggas - 1.0) / m.ggas / m.k_poly, 1.0 / (m.ggas - 1.0));
@@ -541,7 +551,7 @@ __global__ void __launch_bounds__(256) k_torus_cells(Box b, Tabs T, TorusK m, do
     const int j = (int)(t % b.SX) - 2, k = (int)((t / b.SX) % b.SY) - 2, l = (int)(t / ((long long)b.SX * b.SY)) - 2;
     double v[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, e = 0.0;
     if (j >= 1 && j <= b.nx && k >= 1 && k <= b.ny && l >= 1 && l <= b.nz)
-        torus_cell(T, m, j, k, v[IRHO], v[IVZ], v[ITAU], e);
+        torus_cell(T, m, j, k, l, v[IRHO], v[m.cyl ? IVY : IVZ], v[ITAU], e);
 #pragma unroll
     for (int q = 0; q < 8; ++q) prim[8 * t + q] = v[q];
     eps[t] = e;
@@ -559,24 +569,32 @@ __device__ __forceinline__ double torus_corner(const Box& b, const TorusK& m, co
     return 0.25 * (((A(j, l) + A(j + 1, l)) + A(j, l + 1)) + A(j + 1, l + 1));
 }
 
-// face fields on 0:n (model.f90:153-162): B = curl(A_phi)
+// face fields on 0:n, B = curl(A_phi): spherical (model/torus_sph/src/
+// model.f90:153-162) B_r, B_theta; cylindrical (model/torus_cyn/src/
+// model.f90:149-158) B_R = -dA/dz, B_z = d(R A)/(R dR)
 __global__ void __launch_bounds__(256) k_torus_faces(Box b, Tabs T, TorusK m, double* prim) {
     const long long n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n0 * n1 * n2) return;
     const int j = (int)(t % n0), k = (int)((t / n0) % n1), l = (int)(t / (n0 * n1));
     const double a = torus_corner(b, m, prim, j, k, l);
-    const double akm = torus_corner(b, m, prim, j, k - 1, l);
     const double ajm = torus_corner(b, m, prim, j - 1, k, l);
     const double xfj = T.ax[0].f[j], xfjm = T.ax[0].f[j - 1];
     const long long i = b.idx(j, k, l);
-    prim[8 * i + IBX] = (T.sinf[k] * a - T.sinf[k - 1] * akm) / (xfj * T.dcos[k]);
-    prim[8 * i + IBY] = -(xfj * a - xfjm * ajm) / (T.ax[0].c[j] * T.ax[0].d[j]);
+    if (m.cyl) {
+        const double alm = torus_corner(b, m, prim, j, k, l - 1);
+        prim[8 * i + IBX] = -(a - alm) / T.ax[2].d[l];
+        prim[8 * i + IBZ] = (xfj * a - xfjm * ajm) / (T.ax[0].c[j] * T.ax[0].d[j]);
+    } else {
+        const double akm = torus_corner(b, m, prim, j, k - 1, l);
+        prim[8 * i + IBX] = (T.sinf[k] * a - T.sinf[k - 1] * akm) / (xfj * T.dcos[k]);
+        prim[8 * i + IBY] = -(xfj * a - xfjm * ajm) / (T.ax[0].c[j] * T.ax[0].d[j]);
+    }
 }
 
 // maxima of p and of the cell magnetic pressure over the active cells
 // (model.f90:176-219), as 64-bit patterns of non-negative doubles
-__global__ void __launch_bounds__(256) k_torus_max(Box b, const double* prim, unsigned long long* mx) {
+__global__ void __launch_bounds__(256) k_torus_max(Box b, TorusK m, const double* prim, unsigned long long* mx) {
     const long long total = (long long)b.nx * b.ny * b.nz;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double pg = 0.0, pm = 0.0;
@@ -584,9 +602,12 @@ __global__ void __launch_bounds__(256) k_torus_max(Box b, const double* prim, un
         const int j = (int)(t % b.nx) + 1, k = (int)((t / b.nx) % b.ny) + 1, l = (int)(t / ((long long)b.nx * b.ny)) + 1;
         const long long i = b.idx(j, k, l);
         const double bcx = 0.5 * (prim[8 * i + IBX] + prim[8LL * b.idx(j - 1, k, l) + IBX]);
-        const double bcy = 0.5 * (prim[8 * i + IBY] + prim[8LL * b.idx(j, k - 1, l) + IBY]);
+        // the second field: B_theta (spherical); B_z averaged over the phi
+        // neighbour, as model/torus_cyn/src/model.f90:166 does (cylindrical)
+        const int q2 = m.cyl ? IBZ : IBY;
+        const double bc2 = 0.5 * (prim[8 * i + q2] + prim[8LL * b.idx(j, k - 1, l) + q2]);
         pg = prim[8 * i + ITAU];
-        pm = 0.5 * (bcx * bcx + bcy * bcy);
+        pm = 0.5 * (bcx * bcx + bc2 * bc2);
     }
 #pragma unroll
     for (int s = 16; s > 0; s >>= 1) {
@@ -609,7 +630,7 @@ __global__ void __launch_bounds__(256) k_torus_finish(Box b, TorusK m, const uns
         const double pg = __longlong_as_double((long long)mx[0]), pm = __longlong_as_double((long long)mx[1]);
         const double norm = pm > 0.0 ? sqrt((pg / pm) / m.beta) : 0.0;
         prim[8 * t + IBX] *= norm;
-        prim[8 * t + IBY] *= norm;
+        prim[8 * t + (m.cyl ? IBZ : IBY)] *= norm;
     }
     if (j >= 1 && j <= b.nx && k >= 1 && k <= b.ny && l >= 1 && l <= b.nz) {
         const unsigned long long idx =
@@ -1675,9 +1696,12 @@ extern "C" int cumc_restore_state(cumc_ctx* c, const double* host_state) {
 // ---------------------------------------------------------------------------
 extern "C" int cumc_model_torus(cumc_ctx* c, const cumc_torus_model* p) {
     if (!c || !p) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
-    if (c->coord != CUMC_SPHERICAL) return c->fail(CUMC_ERR_CONFIG, "the torus model needs CUMC_SPHERICAL");
+    if (c->coord == CUMC_CARTESIAN)
+        return c->fail(CUMC_ERR_CONFIG, "the torus model needs CUMC_SPHERICAL or CUMC_CYLINDRICAL");
     const double g = c->ggas, q = p->q_grad, rsh = p->r_sh;
-    auto schw = [&](double r) { return -1.0 / (r - rsh); };
+    const bool cyl = c->coord == CUMC_CYLINDRICAL;
+    // the potential on the equator (z = 0 for the cylindrical form)
+    auto schw = [&](double r) { return cyl ? -1.0 / (std::sqrt(r * r + 0.0 * 0.0) - rsh) : -1.0 / (r - rsh); };
     TorusK m;
     m.ggas = g;
     m.r_sh = rsh;
@@ -1695,6 +1719,7 @@ extern "C" int cumc_model_torus(cumc_ctx* c, const cumc_torus_model* p) {
     m.noise = p->noise;
     m.rho_floor = p->rho_fac * p->rho_max;
     m.seed = p->seed;
+    m.cyl = cyl ? 1 : 0;
     int rc = ensure_staging(c);
     if (rc != CUMC_OK) return rc;
     if (!c->model_max && (rc = dalloc(c, &c->model_max, 2)) != CUMC_OK) return rc;
@@ -1705,7 +1730,7 @@ extern "C" int cumc_model_torus(cumc_ctx* c, const cumc_torus_model* p) {
     launch(c, -1, (long long)NT, 256, k_torus_cells, b, c->tabs, m, prim, eps);
     launch(c, -1, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_torus_faces, b, c->tabs, m, prim);
     CUMC_CHECK(cudaMemsetAsync(c->model_max, 0, 2 * sizeof(unsigned long long), c->stream));
-    launch(c, -1, (long long)b.nx * b.ny * b.nz, 256, k_torus_max, b, (const double*)prim, c->model_max);
+    launch(c, -1, (long long)b.nx * b.ny * b.nz, 256, k_torus_max, b, m, (const double*)prim, c->model_max);
     launch(c, -1, (long long)NT, 256, k_torus_finish, b, m, (const unsigned long long*)c->model_max, prim);
     if (!c->mixed) {  // the FP64 state arrays, as cumc_upload_state fills them
         double* dst[9] = {c->w[0], c->w[1], c->w[2], c->w[3], c->w[4],

@@ -371,7 +371,7 @@ def torus_cyl(nr: int = 32, nph: int = 8, nz: int = 32, ggas: float = 5.0 / 3.0,
               r_in: float = 1.5, r_out: float = 8.0, z_half: float = 3.0, r_sh: float = 1.0, s_in: float = 3.0,
               s_max: float = 4.7, q_grad: float = 2.0, rho_max: float = 1.0, rho_fac: float = 1.0e-4,
               rho_cut: float = 0.5, beta: float = 100.0, noise: float = 1.0e-4, seed: int = 4,
-              geom_source_repeat: int = 8) -> Problem:
+              geom_source_repeat: int = 8, host_arrays: bool = True) -> Problem:
     """Magnetised torus on a cylindrical grid (R, phi, z), following
     model/torus_cyn/src/model.f90:8-284: the pseudo-Newtonian potential
     -1/(sqrt(R^2 + z^2) - r_sh), angular momentum l^2 ~ R^(2-2q) from the
@@ -382,7 +382,9 @@ def torus_cyl(nr: int = 32, nph: int = 8, nz: int = 32, ggas: float = 5.0 / 3.0,
     normalised to p_gas,max / p_mag,max = beta (the cell B_z of that ratio
     averages over the phi neighbour, as model.f90:166 does); then seeded
     density noise rho (1 + noise (2u - 1)) where rho > rho_floor. Faces:
-    outflow in R and z (the model's ghost clamps apply there), periodic in phi."""
+    outflow in R and z (the model's ghost clamps apply there), periodic in phi.
+    With host_arrays=False only the grid and configuration are built; the
+    device-side generator (CUMC3D.generate_model) then builds the state."""
     xf = uniform_faces(r_in, r_out, nr)
     yf = uniform_faces(0.0, 2.0 * math.pi, nph)
     zf = uniform_faces(-z_half, z_half, nz)
@@ -397,6 +399,14 @@ def torus_cyl(nr: int = 32, nph: int = 8, nz: int = 32, ggas: float = 5.0 / 3.0,
     k_poly = h_max * (ggas - 1.0) / ggas / rho_max ** (ggas - 1.0)
     if k_poly < 0.0:
         raise ValueError("the polytropic constant is negative")
+    params = dict(r_sh=r_sh, s_in=s_in, s_max=s_max, q_grad=q_grad, rho_max=rho_max, rho_fac=rho_fac,
+                  rho_cut=rho_cut, beta=beta, noise=noise, seed=seed)
+    if not host_arrays:
+        rho_floor = rho_fac * rho_max
+        return Problem(f"torus_cyl_{nr}x{nph}x{nz}", nr, nph, nz, xf, yf, zf, N.CYLINDRICAL, (1, 1, 0, 0, 1, 1),
+                       ggas, cfl, 0.0, None, None, model=N.MODEL_TORUS_CYN, rho_floor=rho_floor,
+                       eps_floor=k_poly * rho_floor ** (ggas - 1.0) / (ggas - 1.0), r_sh=r_sh,
+                       geom_source_repeat=geom_source_repeat, model_params=params)
     R = _centres(xf)[3:nr + 3][None, None, :]
     Z = _centres(zf)[3:nz + 3][:, None, None]
     h = -schw(R, Z) + lkep2 * R ** (2.0 - 2.0 * q_grad) / (2.0 - 2.0 * q_grad) + c_const
@@ -444,4 +454,4 @@ def torus_cyl(nr: int = 32, nph: int = 8, nz: int = 32, ggas: float = 5.0 / 3.0,
     prim[sl1 + (IRHO,)] = np.where(d > rho_floor, d + d * (u - 0.5) / 0.5 * noise, d)
     return Problem(f"torus_cyl_{nr}x{nph}x{nz}", nr, nph, nz, xf, yf, zf, N.CYLINDRICAL, (1, 1, 0, 0, 1, 1), ggas,
                    cfl, 0.0, prim, eps, model=N.MODEL_TORUS_CYN, rho_floor=rho_floor, eps_floor=eps_floor,
-                   r_sh=r_sh, geom_source_repeat=geom_source_repeat)
+                   r_sh=r_sh, geom_source_repeat=geom_source_repeat, model_params=params)

@@ -177,17 +177,19 @@ int cumc_profile_read(cumc_ctx* ctx, int which, int* launches, double* ms);
 /* Number of kernel launches the library issued since cumc_init. */
 int cumc_launch_count(cumc_ctx* ctx, long long* count);
 
-/* Device-side GET_MODEL of the spherical torus (model/torus_sph/src/
- * model.f90:8-284), for grids too large to build on the host: a
- * constant-angular-momentum torus around a point mass at r_sh (potential
- * -1/(r - r_sh)), polytropic with p = K rho^gamma, density floor
- * rho_fac * rho_max outside; A_phi = max(rho - rho_cut, 0)/rho_max on the
- * cells, averaged to the corners, face fields B = curl A normalised to
- * max p_gas / max p_mag = beta; then density noise rho (1 + noise (2u - 1))
- * where rho > rho_fac * rho_max, u from splitmix64(seed, linear cell index).
- * Fills the state as cumc_upload_state would (call cumc_initial_update
- * next); the grid is the context's (CUMC_SPHERICAL, else CUMC_ERR_CONFIG).
- * The host generator cumpic_b200.problems.torus builds the same state. */
+/* Device-side GET_MODEL of the tori (model/torus_sph/src/model.f90:8-284 on
+ * a CUMC_SPHERICAL grid, model/torus_cyn/src/model.f90:8-284 on a
+ * CUMC_CYLINDRICAL one), for grids too large to build on the host: a
+ * constant-angular-momentum torus, potential -1/(r - r_sh) (spherical) or
+ * -1/(sqrt(R^2 + z^2) - r_sh) (cylindrical), polytropic with
+ * p = K rho^gamma, density floor rho_fac * rho_max outside;
+ * A_phi = max(rho - rho_cut, 0)/rho_max on the cells, averaged to the
+ * corners, face fields B = curl A normalised to max p_gas / max p_mag = beta;
+ * then density noise rho (1 + noise (2u - 1)) where rho > rho_fac * rho_max,
+ * u from splitmix64(seed, linear cell index). Fills the state as
+ * cumc_upload_state would (call cumc_initial_update next); the grid is the
+ * context's (CUMC_ERR_CONFIG on a Cartesian one). The host generators
+ * cumpic_b200.problems.torus and torus_cyl build the same states. */
 typedef struct {
     double r_sh, s_in, s_max, q_grad;   /* potential centre, torus inner edge, pressure maximum, l ~ s^(2-q) */
     double rho_max, rho_fac, rho_cut;   /* peak density, floor factor, field threshold */
