@@ -1,8 +1,8 @@
 """Mixed-precision path (CUMC_MIXED) against the FP64 path.
 
-Bars: relative L1 of the density against the FP64 run <= 1e-5 (the
-north-star's bar for the mixed form) and the normalised max |div B| of the
-compensated face fields at round-off.
+Bars: relative L1 of the density against the FP64 run <= 1e-5 (the accuracy
+bar of the mixed form) and the normalised max |div B| of the compensated face
+fields at round-off.
 """
 import numpy as np
 import pytest

@@ -3,7 +3,7 @@
 The FP64 path is compiled without FMA contraction and evaluates every
 expression in the reference's order, so on the small cases below it must agree
 with the oracle bit for bit (max |diff| == 0). The full Brio-Wu run is checked
-against the survey's bar, relative L1 <= 1e-10 per conserved variable.
+against the FP64 parity bar: relative L1 <= 1e-10 per conserved variable.
 """
 import numpy as np
 import pytest
@@ -15,7 +15,7 @@ from compare import diffs, rel_l1_interior
 pytestmark = pytest.mark.gpu
 
 BITWISE = 0.0
-REL_L1_TOL = 1.0e-10  # FP64 bar of the survey (per conserved variable, at t_end)
+REL_L1_TOL = 1.0e-10  # FP64 parity bar (per conserved variable, at t_end)
 
 
 def _pair(problem, threads=8):
