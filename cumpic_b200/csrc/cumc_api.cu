@@ -87,7 +87,8 @@ struct cumc_ctx {
     void* adj_slab = nullptr;       // adjoint scratch, kept between runs
     size_t adj_slab_bytes = 0;
     int next_stage = 1;    // cumc_rk_stage: the stage due next
-    bool fuse_dt = false;  // cumc_advance: stage 3 also forms the next step's CFL dt
+    bool fuse_dt = false;  // stage 3 also forms the next step's CFL dt (cumc_advance, cumc_rungekutta)
+    bool dt_valid = false; // dtmin holds the CFL dt of the current state (set by cumc_rungekutta only)
     int bf_set = 0;        // U[bf_set] holds the current face fields (the last stage's output)
     bool exchange = false;  // a z face is CUMC_BC_EXCHANGE
     unsigned long long* model_max = nullptr;  // cumc_model_torus: the two maxima
@@ -954,6 +955,7 @@ static int get_soa(cumc_ctx* c, double* host, int nv, const double* const* srcp)
 }
 
 int cumc_upload_state(cumc_ctx* c, const double* prim, const double* eps) {
+    if (c) c->dt_valid = false;  // the state changes: the cached CFL dt is stale
     if (!c || !prim || !eps) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
     if (c->mixed) {  // kept as FP64 AoS until cumc_initial_update converts it
         const size_t NT = (size_t)c->box.count();
@@ -1014,6 +1016,7 @@ int cumc_download_state(cumc_ctx* c, double* prim, double* cons, double* eps, do
 }
 
 int cumc_initial_update(cumc_ctx* c) {
+    if (c) c->dt_valid = false;  // the state changes: the cached CFL dt is stale
     if (!c) return CUMC_ERR_ARG;
     if (!c->uploaded) return c->fail(CUMC_ERR_STATE, "cumc_upload_state must come first");
     if (c->mixed) {
@@ -1034,7 +1037,7 @@ int cumc_finddt(cumc_ctx* c, double* dt) {
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
     if (!dt) return c->fail(CUMC_ERR_ARG, "null dt");
-    finddt_launch(c, c->box);
+    if (!c->dt_valid) finddt_launch(c, c->box);  // else the last cumc_rungekutta's stage 3 formed it
     CUMC_CHECK(cudaMemcpyAsync(c->host_pinned, c->dtmin, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     CUMC_CHECK(cudaMemcpyAsync(c->host_pinned + 1, c->flag_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
     CUMC_CHECK(cudaStreamSynchronize(c->stream));
@@ -1052,11 +1055,18 @@ int cumc_rungekutta(cumc_ctx* c, double dt) {
     if (c->exchange) return c->fail(CUMC_ERR_STATE, "a slab with CUMC_BC_EXCHANGE faces steps by cumc_rk_stage and the halo exchange");
     if (c->next_stage != 1) return c->fail(CUMC_ERR_STATE, "cumc_rk_stage left a step unfinished");
     launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
+    // stage 3 forms the next step's CFL dt, which cumc_finddt then returns
+    // without a pass over the state (the same expression, so the same bits)
+    launch(c, -1, 1, 1, k_reset_dtmin, c->dtmin);
+    c->fuse_dt = true;
     rk_step(c, c->box);
+    c->fuse_dt = false;
+    c->dt_valid = true;
     return sync_status(c);
 }
 
 int cumc_rk_stage(cumc_ctx* c, int stage, double dt) {
+    if (c) c->dt_valid = false;  // the state changes: the cached CFL dt is stale
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
     if (stage != c->next_stage) return c->fail(CUMC_ERR_STATE, "stage %d called where stage %d is due", stage, c->next_stage);
@@ -1092,9 +1102,13 @@ static int halo_copy(cumc_ctx* c, int side, double* buf, bool pack) {
 }
 
 int cumc_halo_pack(cumc_ctx* c, int side, double* buf) { return halo_copy(c, side, buf, true); }
-int cumc_halo_unpack(cumc_ctx* c, int side, const double* buf) { return halo_copy(c, side, const_cast<double*>(buf), false); }
+int cumc_halo_unpack(cumc_ctx* c, int side, const double* buf) {
+    if (c) c->dt_valid = false;
+    return halo_copy(c, side, const_cast<double*>(buf), false);
+}
 
 int cumc_spatial(cumc_ctx* c) {
+    if (c) c->dt_valid = false;  // the state changes: the cached CFL dt is stale
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
     if (c->mixed) return c->fail(CUMC_ERR_STATE, "cumc_spatial is available for CUMC_FP64 only");
@@ -1151,6 +1165,7 @@ int cumc_divb(cumc_ctx* c, double* maxdb_signed, double* maxabs_norm) {
 }
 
 int cumc_advance(cumc_ctx* c, int nsteps, double t_end, double* t_inout, int* steps_done) {
+    if (c) c->dt_valid = false;  // the state changes: the cached CFL dt is stale
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
     if (c->exchange) return c->fail(CUMC_ERR_STATE, "a slab with CUMC_BC_EXCHANGE faces steps by cumc_rk_stage and the halo exchange");
@@ -1609,6 +1624,7 @@ int adjoint_run(cumc_ctx* c, int N, int K, int obj, const double* weights, const
 
 extern "C" int cumc_adjoint_run(cumc_ctx* c, int nsteps, int checkpoint_every, int objective, const double* weights,
                                 const double* dt_in, double* dt_out, double* J, double* grad_prim, double* grad_eps) {
+    if (c) c->dt_valid = false;
     if (!c) return CUMC_ERR_ARG;
     if (!c->uploaded) return c->fail(CUMC_ERR_STATE, "cumc_upload_state must come first");
     if (c->mixed || c->exchange || (c->model != CUMC_MODEL_NONE && c->model != CUMC_MODEL_RIEMANN))
@@ -1674,6 +1690,7 @@ extern "C" int cumc_snapshot_wait(cumc_ctx* c) {
 }
 
 extern "C" int cumc_restore_state(cumc_ctx* c, const double* host_state) {
+    if (c) c->dt_valid = false;  // the state changes: the cached CFL dt is stale
     if (!c || !host_state) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
     if (c->mixed) return c->fail(CUMC_ERR_CONFIG, "snapshots cover CUMC_FP64");
     int rc = cumc_snapshot_wait(c);  // the staging slab and stream are quiet
@@ -1695,6 +1712,7 @@ extern "C" int cumc_restore_state(cumc_ctx* c, const double* host_state) {
 // cumc_model_torus: GET_MODEL of the spherical torus on the device
 // ---------------------------------------------------------------------------
 extern "C" int cumc_model_torus(cumc_ctx* c, const cumc_torus_model* p) {
+    if (c) c->dt_valid = false;  // the state changes: the cached CFL dt is stale
     if (!c || !p) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
     if (c->coord == CUMC_CARTESIAN)
         return c->fail(CUMC_ERR_CONFIG, "the torus model needs CUMC_SPHERICAL or CUMC_CYLINDRICAL");
