@@ -11,6 +11,8 @@
 #include "cumc_walk.cuh"
 #include "cumc_adjoint.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <cmath>
 #include <type_traits>
 #include <cstdarg>
@@ -409,7 +411,15 @@ Launcher mx_launcher(cumc_ctx* c) { return Launcher{c->stream, mx_pre, mx_post, 
 
 // One SPATIAL + combine + conversions + boundary (solver/rungekutta.f90:38-66).
 // stage 0: SPATIAL only, l_rk stored in c->L.
+// an NVTX range for the scope (shown by Nsight tools; a no-op without one)
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+
 void run_stage(cumc_ctx* c, const Box& b, int stage) {
+    static const char* const names[4] = {"cumc spatial", "cumc rk stage 1", "cumc rk stage 2", "cumc rk stage 3"};
+    const NvtxRange range(names[stage]);
     if (c->mixed) {
         if (stage > 0)
             mixed_stage(mx_launcher(c), b, c->tabs, c->mb, c->mp, stage, stage == 3 && c->fuse_dt ? c->dtmin : nullptr);
@@ -1054,6 +1064,7 @@ int cumc_rungekutta(cumc_ctx* c, double dt) {
     if (rc != CUMC_OK) return rc;
     if (c->exchange) return c->fail(CUMC_ERR_STATE, "a slab with CUMC_BC_EXCHANGE faces steps by cumc_rk_stage and the halo exchange");
     if (c->next_stage != 1) return c->fail(CUMC_ERR_STATE, "cumc_rk_stage left a step unfinished");
+    if (!(dt >= 0.0 && std::isfinite(dt))) return c->fail(CUMC_ERR_ARG, "dt must be finite and non-negative");
     launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
     // stage 3 forms the next step's CFL dt, which cumc_finddt then returns
     // without a pass over the state (the same expression, so the same bits)
@@ -1070,6 +1081,8 @@ int cumc_rk_stage(cumc_ctx* c, int stage, double dt) {
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
     if (stage != c->next_stage) return c->fail(CUMC_ERR_STATE, "stage %d called where stage %d is due", stage, c->next_stage);
+    if (stage == 1 && !(dt >= 0.0 && std::isfinite(dt)))
+        return c->fail(CUMC_ERR_ARG, "dt must be finite and non-negative");
     if (stage == 1) launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
     run_stage(c, c->box, stage);
     c->next_stage = stage == 3 ? 1 : stage + 1;
@@ -1632,6 +1645,10 @@ extern "C" int cumc_adjoint_run(cumc_ctx* c, int nsteps, int checkpoint_every, i
     if (nsteps < 1 || checkpoint_every < 1) return c->fail(CUMC_ERR_ARG, "nsteps and checkpoint_every must be >= 1");
     if (objective < CUMC_OBJ_MAGNETIC || objective > CUMC_OBJ_LINEAR) return c->fail(CUMC_ERR_ARG, "unknown objective");
     if (objective == CUMC_OBJ_LINEAR && !weights) return c->fail(CUMC_ERR_ARG, "CUMC_OBJ_LINEAR needs weights");
+    if (dt_in)
+        for (int n = 0; n < nsteps; ++n)
+            if (!(dt_in[n] >= 0.0 && std::isfinite(dt_in[n])))
+                return c->fail(CUMC_ERR_ARG, "dt_in[%d] must be finite and non-negative", n);
     const int rc = adjoint_run(c, nsteps, std::min(checkpoint_every, nsteps), objective, weights, dt_in, dt_out, J,
                                grad_prim, grad_eps);
     c->tape = nullptr;

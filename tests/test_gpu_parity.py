@@ -172,6 +172,17 @@ def test_call_order_and_config_errors():
     with pytest.raises(N.CumcError) as e:
         CUMC3D(q)
     assert e.value.code == N.CUMC_ERR_CONFIG
+    # a dt that is negative or not finite is refused; the state is left as it was
+    g.upload()
+    g.initial_update()
+    before = g.download()
+    for bad in (-1e-3, float("nan"), float("inf")):
+        with pytest.raises(N.CumcError) as e:
+            g.rungekutta(bad)
+        assert e.value.code == N.CUMC_ERR_ARG
+    after = g.download()
+    assert all(np.array_equal(before[k], after[k]) for k in before)
+    g.rungekutta(0.0)  # a zero step is allowed
 
 
 @pytest.mark.parametrize("precision", [N.FP64, N.MIXED])
