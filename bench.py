@@ -46,10 +46,14 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-snapshot", action="store_true")
-    ap.add_argument("--adjoint-check", action="store_true",
-                    help="also run the full finite-difference check of the adjoint (128^3, 200 steps, 16 directions)")
+    ap.add_argument("--no-adjoint-check", action="store_true",
+                    help="skip the finite-difference check of the adjoint (128^3, 200 steps, 16 directions)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip Orszag-Tang 512^3 (FP64, mixed) and the torus over 2000 steps (FP64, mixed)")
     ap.add_argument("--all-configs", action="store_true",
-                    help="also run Orszag-Tang 512^3 (mixed vs FP64) and the torus over 2000 steps (FP64, mixed)")
+                    help="compare the 512^3 mixed run with the FP64 run at t_end = 0.5 instead of t = 0.05")
+    ap.add_argument("--no-ref-translation", action="store_true",
+                    help="skip the second CPU figure (the reference's own loop structure)")
     return ap.parse_args()
 
 
@@ -192,15 +196,18 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(n: int, nz: int, steps: int, warmup: int, threads: int | None = None):
-    """FP64 CPU restatement on an Orszag-Tang slab of n x n x nz cells at the
-    bench resolution (cell size 1/n); returns (Mcell-upd/s, threads, seconds)."""
+WORKLOAD = "orszag_tang_3d n={n} fp64 ppm/hll/ct/rk3 cfl=0.4"
+
+
+def cpu_port_rate(n: int, steps: int, warmup: int, threads: int | None = None):
+    """FP64 CPU restatement (OpenMP, all host threads) on the full n^3
+    Orszag-Tang box; returns (Mcell-upd/s, threads, seconds of the timed steps)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from cumpic_b200 import problems as P
     from _oracle import Oracle
 
     threads = threads or os.cpu_count() or 1
-    p = P.orszag_tang(n, nz=nz)
+    p = P.orszag_tang(n)
     o = Oracle(p, threads=threads)
     used = o._L.orc_get_threads()
     o.upload()
@@ -211,30 +218,111 @@ def cpu_reference_rate(n: int, nz: int, steps: int, warmup: int, threads: int | 
     for _ in range(steps):
         o.step()
     el = time.perf_counter() - t0
+    o.close()
     return p.cells * steps / el / 1e6, used, el
 
 
-def calibrate_slab(n: int, seconds_per_step: float, threads: int | None = None) -> int:
-    rate, _, _ = cpu_reference_rate(32, 32, 1, 1, threads)  # Mcell-upd/s at a small size
-    nz = int(rate * 1e6 * seconds_per_step / (n * n))
-    return max(4, min(n, nz))
+def _ref_worker(slab, steps, warmup, go, out):
+    """one host rank of the translated reference: its own periodic
+    Orszag-Tang slab, warm-up, then the timed steps once every rank is ready"""
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from cumpic_b200 import problems as P
+    from _oracle import Oracle, ref_lib_path
+
+    nx, ny, nz = slab
+    o = Oracle(P.orszag_tang(nx, ny=ny, nz=nz), lib_path=ref_lib_path("riemann"))
+    o.upload()
+    o.initial_update()
+    for _ in range(warmup):
+        o.step()
+    out.put(("ready", 0.0))
+    go.wait()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step()
+    out.put(("done", time.perf_counter() - t0))
+
+
+def ref_translation_available() -> bool:
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _oracle import ref_lib_path
+    return os.path.exists(ref_lib_path("riemann"))
+
+
+def cpu_ref_rate(steps: int, warmup: int, slab=(128, 128, 16), procs: int | None = None):
+    """The reference's own loop structure on the host cores: the mechanical
+    C translation of its Fortran (single-threaded, one configuration per
+    process, as one MPI rank of the reference is), run as `procs` spawned
+    processes that each advance their own slab, the way the reference's MPI
+    ranks each advance a subdomain (without the halo exchange, which would
+    only add time). Returns (Mcell-upd/s of all processes over the slowest
+    one's time, processes, seconds)."""
+    import multiprocessing as mp
+    procs = procs or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    go = ctx.Event()
+    out = ctx.Queue()
+    ps = [ctx.Process(target=_ref_worker, args=(slab, steps, warmup, go, out)) for _ in range(procs)]
+    for p in ps:
+        p.start()
+
+    def collect(kind):
+        # one message of `kind` from every rank, giving up as soon as one has died
+        import queue
+        got = []
+        while len(got) < procs:
+            try:
+                k, v = out.get(timeout=5)
+            except queue.Empty:
+                if any(p.exitcode not in (None, 0) for p in ps):
+                    for p in ps:
+                        if p.is_alive():
+                            p.terminate()
+                    raise RuntimeError(f"a reference rank exited before it was {kind}")
+                continue
+            assert k == kind, (k, kind)
+            got.append(v)
+        return got
+
+    collect("ready")
+    go.set()
+    times = collect("done")
+    for p in ps:
+        p.join()
+    el = max(times)
+    cells = slab[0] * slab[1] * slab[2]
+    return procs * cells * steps / el / 1e6, procs, el
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the reference's CPU implementation of the hot path
+    on all host cores (the mechanical translation of its own Fortran, one
+    process per core; the FP64 restatement with OpenMP where the translation
+    is absent), each step a bounded sample of the 256^3 workload."""
     if rank != 0:
         return 0
     n = args.n
-    budget = 150.0  # seconds for warmup + steps
-    nz = calibrate_slab(n, budget / max(1, args.steps + args.warmup))
-    rate, threads, el = cpu_reference_rate(n, nz, args.steps, args.warmup)
+    if ref_translation_available():
+        slab = (128, 128, 16)
+        rate, procs, el = cpu_ref_rate(args.steps, args.warmup, slab)
+        base = {"value": rate, "unit": UNIT, "cores": procs, "kind": "reference",
+                "sample": f"{procs} processes x one {slab[0]}x{slab[1]}x{slab[2]} periodic Orszag-Tang slab each "
+                          f"({slab[0] * slab[1] * slab[2]} cells a process; a {n}^3 box split over {procs} MPI ranks "
+                          f"gives each {n ** 3 // procs}), {args.steps} RK3 steps after {args.warmup} warm-up; "
+                          f"mechanical C translation of the reference's Fortran (oracle/f2c_ref.py), "
+                          f"single-threaded per process, gcc -O2"}
+    else:
+        rate, threads, el = cpu_port_rate(n, args.steps, args.warmup)
+        base = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                "sample": f"Orszag-Tang {n}^3, {args.steps} RK3 steps after {args.warmup} warm-up "
+                          f"(FP64 C++ restatement, OpenMP)"}
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"orszag_tang_3d n={n} fp64 ppm/hll/ct/rk3", "sample": f"{n}x{n}x{nz} slab, cell size 1/{n}"},
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"Orszag-Tang {n}x{n}x{nz} slab at cell size 1/{n}, {args.steps} RK3 steps "
-                                   f"after {args.warmup} warm-up (FP64 C++ restatement, OpenMP)"},
+        "config": {"workload": WORKLOAD.format(n=n), "sample": base["sample"]},
+        "cpu_baseline": base,
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -246,7 +334,8 @@ def mixed_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> d
     """The mixed form (CUMC_MIXED) on the same workload: throughput, its ratio
     to the FP64 path, and its relative L1 error per conserved variable and
     normalised max |div B| against the FP64 path (bit-identical to the FP64
-    oracle) at t = 0.05, for B as given and B x 10 (plasma beta ~0.05)."""
+    oracle) at the configuration's t_end = 0.5, for B as given and B x 10
+    (plasma beta ~0.05)."""
     import torch
     from cumpic_b200 import _native as NN
     from cumpic_b200 import problems as P
@@ -269,7 +358,7 @@ def mixed_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> d
     ms = e0.elapsed_time(e1)
     sim.close()
     out = {"value": prob.cells * steps / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms / steps,
-           "speedup_vs_fp64": fp64_ms_per_step / (ms / steps), "accuracy_t": 0.05, "vs_fp64": {}}
+           "speedup_vs_fp64": fp64_ms_per_step / (ms / steps), "accuracy_t": prob.t_end, "vs_fp64": {}}
     names = ("rho", "mx", "my", "mz", "E", "bx", "by", "bz")
     for bscale in (1.0, 10.0):
         res = {}
@@ -277,12 +366,14 @@ def mixed_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> d
             s = CUMC3D(P.orszag_tang(n, bscale=bscale, precision=prec))
             s.upload()
             s.initial_update()
-            s.run(0.05)
-            res[prec] = (s.download(), s.find_divb()[1])
+            steps_run = s.run(prob.t_end)
+            res[prec] = (s.download(), s.find_divb()[1], steps_run)
             s.close()
         rel = rel_l1_interior(res[NN.MIXED][0], res[NN.FP64][0])
         out["vs_fp64"][f"bscale_{bscale:g}"] = {"rel_l1": {k: rel[q] for q, k in enumerate(names)},
-                                                "max_divb_norm": res[NN.MIXED][1]}
+                                                "max_divb_norm": res[NN.MIXED][1],
+                                                "max_divb_norm_fp64": res[NN.FP64][1],
+                                                "steps": {"fp64": res[NN.FP64][2], "mixed": res[NN.MIXED][2]}}
     return out
 
 
@@ -375,11 +466,13 @@ def adjoint_section(n: int = 128, steps: int = 200, ckpt: int = 20) -> dict:
                     "initial_update and the same steps with the same dt"}
 
 
-def config_runs() -> dict:
-    """The remaining configurations: Orszag-Tang 512^3 in the mixed form
-    against FP64 (t = 0.05), and the spherical torus 192 x 128 x 64 over 2000
-    steps in FP64 and in the mixed form (throughput, the mixed run's relative
-    L1 against the FP64 run, both runs' normalised max |div B|)."""
+def config_runs(t512: float = 0.05) -> dict:
+    """The remaining configurations: Orszag-Tang 512^3, FP64 and mixed
+    (throughput over 10 device-loop steps after 2 warm-up, then the mixed
+    run's relative L1 per variable and both runs' normalised max |div B|
+    against the FP64 run at t = t512), and the spherical torus 192 x 128 x 64
+    over 2000 steps in FP64 and in the mixed form (throughput, the mixed run's
+    relative L1 against the FP64 run, both runs' normalised max |div B|)."""
     import torch
     from cumpic_b200 import _native as NN
     from cumpic_b200 import problems as P
@@ -400,20 +493,30 @@ def config_runs() -> dict:
 
     out = {}
     res = {}
+    rate512 = {}
     for prec in (NN.FP64, NN.MIXED):
         prob = P.orszag_tang(512, precision=prec)
         s = CUMC3D(prob)
         s.upload()
         s.initial_update()
-        ms = timed(s, lambda: s.run(0.05))
-        res[prec] = (s.download(), s.find_divb()[1], prob.cells * s.n_step / (ms / 1e3) / 1e6, s.n_step)
+        s.advance(2)
+        ms = timed(s, lambda: s.advance(10))
+        rate512[prec] = prob.cells * 10 / (ms / 1e3) / 1e6
+        s.upload()
+        s.initial_update()
+        s.global_time, s.n_step = 0.0, 0
+        s.run(t512)
+        res[prec] = (s.download(), s.find_divb()[1], s.n_step)
         s.close()
+        del s
     rel = rel_l1_interior(res[NN.MIXED][0], res[NN.FP64][0])
-    out["orszag_tang_512_t0.05"] = {
-        "fp64_mcell_upd_s": res[NN.FP64][2], "mixed_mcell_upd_s": res[NN.MIXED][2],
-        "steps": {"fp64": res[NN.FP64][3], "mixed": res[NN.MIXED][3]},
+    out[f"orszag_tang_512"] = {
+        "fp64_mcell_upd_s": rate512[NN.FP64], "mixed_mcell_upd_s": rate512[NN.MIXED],
+        "mixed_speedup": rate512[NN.MIXED] / rate512[NN.FP64], "accuracy_t": t512,
+        "steps_to_accuracy_t": {"fp64": res[NN.FP64][2], "mixed": res[NN.MIXED][2]},
         "mixed_rel_l1_vs_fp64": {k: rel[q] for q, k in enumerate(names)},
         "max_divb_norm": {"fp64": res[NN.FP64][1], "mixed": res[NN.MIXED][1]}}
+    del res
     # torus: throughput with the device-side dt, then the accuracy runs with
     # the FP64 run's dt sequence replayed by the mixed run (same times)
     rate = {}
@@ -553,7 +656,7 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"orszag_tang_3d n={n} fp64 ppm/hll/ct/rk3 cfl=0.4",
+        "config": {"workload": WORKLOAD.format(n=n),
                    "cells_per_gpu": cells, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (each of the 8 state arrays is %.2f GB)" % (8 * (n + 6) ** 3 / 1e9)},
         "gpu_launches": launches,
@@ -608,11 +711,18 @@ def run_ours(args, world, rank, local):
 
     # ---- CPU baseline: the restatement on the host cores (rank 0, N=1) -------
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        nz = calibrate_slab(n, 6.0)
-        rate, threads, el = cpu_reference_rate(n, nz, 2, 1)
+        rate, threads, el = cpu_port_rate(n, 10, 2)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"Orszag-Tang {n}x{n}x{nz} slab at cell size 1/{n}, 2 RK3 steps after 1 "
-                                          f"warm-up ({el:.1f} s; FP64 C++ restatement, OpenMP)"}
+                                "sample": f"Orszag-Tang {n}^3 (the whole workload), 10 RK3 steps after 2 warm-up "
+                                          f"({el:.1f} s; FP64 C++ restatement, OpenMP)"}
+        if not args.no_ref_translation and ref_translation_available():
+            slab = (128, 128, 16)
+            rrate, procs, rel_s = cpu_ref_rate(3, 1, slab)
+            line["cpu_baseline"]["reference_translation"] = {
+                "value": rrate, "unit": UNIT, "cores": procs, "kind": "reference",
+                "sample": f"{procs} processes x one {slab[0]}x{slab[1]}x{slab[2]} periodic Orszag-Tang slab each, "
+                          f"3 RK3 steps after 1 warm-up ({rel_s:.1f} s); mechanical C translation of the "
+                          f"reference's Fortran, single-threaded per process"}
     sim.close()
     if world == 1 and not args.no_mixed:
         line["mixed"] = mixed_section(n, args.steps, args.warmup, ms_max / args.steps)
@@ -620,10 +730,10 @@ def run_ours(args, world, rank, local):
         line["snapshot"] = snapshot_section(n)
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_section()
-        if args.adjoint_check:
+        if not args.no_adjoint_check:
             line["adjoint"]["fd_check"] = adjoint_check()
-    if world == 1 and args.all_configs:
-        line["configs"] = config_runs()
+    if world == 1 and not args.no_configs:
+        line["configs"] = config_runs(0.5 if args.all_configs else 0.05)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

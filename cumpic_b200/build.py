@@ -66,8 +66,11 @@ def build_oracle(force: bool = False) -> str:
     if force:
         subprocess.run(args + ["clean"], check=True)
     subprocess.run(args, check=True)
-    reference = os.environ.get("CUMC_REFERENCE", "/root/reference")
-    if os.path.isdir(os.path.join(reference, "solver")):
+    # the reference's source tree: CUMC_REFERENCE, else the recipe's default
+    override = [f"REFERENCE={os.environ['CUMC_REFERENCE']}"] if os.environ.get("CUMC_REFERENCE") else []
+    reference = subprocess.run(args + ["print-reference", *override], check=True, capture_output=True,
+                               text=True).stdout.strip()
+    if reference and os.path.isdir(os.path.join(reference, "solver")):
         subprocess.run(args + ["ref", f"REFERENCE={reference}"], check=True)
     return os.path.join(ROOT, "oracle", "build", "libcumc_oracle.so")
 

@@ -215,6 +215,50 @@ __device__ __forceinline__ void hll_flux7(const R wl[8], const R wr[8], R ggas, 
 }
 
 // ---------------------------------------------------------------------------
+// CFL time step of one cell (finddt, solver/rungekutta.f90:201-250)
+// ---------------------------------------------------------------------------
+
+// the fast magnetosonic speed along each axis from the cell's primitives and
+// bcell, then cfl * min(dx, dy, dz) / max_d(|v_d| + c_f,d); the inner square
+// root has no MAX(., 0) guard, as in the reference. dxl, dyl, dzl are the
+// cell's lengths along the three axes (cfl_lengths). Every caller of the CFL
+// step (finddt, its fusion into stage 3, cumc_cfl_dt_static) evaluates this
+// one function, so they give the same double.
+__host__ __device__ __forceinline__ double cfl_cell_dt(double rho, double p, double vx, double vy, double vz,
+                                                       double bcx, double bcy, double bcz, double dxl, double dyl,
+                                                       double dzl, double ggas, double cfl) {
+    const double cs = sqrt((ggas * p) / rho);
+    const double a2 = cs * cs;
+    const double a4 = a2 * a2;
+    const double b2x = (bcx * bcx) / rho;
+    const double b2y = (bcy * bcy) / rho;
+    const double b2z = (bcz * bcz) / rho;
+    const double b2 = (b2x + b2y) + b2z;
+    const double b4 = b2 * b2;
+    const double base = (a4 + (2.0 * a2) * b2) + b4;
+    const double cfx = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2x)));
+    const double cfy = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2y)));
+    const double cfz = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2z)));
+    const double lambda = fmax(fmax(fabs(vx) + cfx, fabs(vy) + cfy), fabs(vz) + cfz);
+    return (fmin(fmin(dxl, dyl), dzl) * cfl) / lambda;
+}
+
+// the cell's lengths along the axes (solver/rungekutta.f90:237-243): the
+// widths, with dy -> r dy on cylindrical and spherical grids and
+// dz -> r sin(theta) dz on spherical ones; xc is the cell-centre radius and
+// sinyc the sine of the polar cell centre. coordinate: 1 Cartesian,
+// 2 cylindrical, 3 spherical.
+__host__ __device__ __forceinline__ void cfl_lengths(int coordinate, double xc, double sinyc, double& dyl,
+                                                     double& dzl) {
+    if (coordinate == 2) {
+        dyl = xc * dyl;
+    } else if (coordinate == 3) {
+        dyl = xc * dyl;
+        dzl = (xc * sinyc) * dzl;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // geometry (solver/coords.f90) from the 1-D tables
 // ---------------------------------------------------------------------------
 

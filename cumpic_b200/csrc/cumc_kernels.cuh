@@ -156,33 +156,14 @@ __global__ void __launch_bounds__(256) k_emf(Box b, PrimT<R> pr, FaceFluxT<R> fx
     out.e[2][i] = ez;
 }
 
-// CFL step of one interior cell (solver/rungekutta.f90:201-250): the fast
-// magnetosonic speed along each axis from the cell's primitives and bcell
+// CFL step of one interior cell (solver/rungekutta.f90:201-250)
 template <int COORD>
 __device__ __forceinline__ double cell_dt(const Tabs& T, int j, int k, int l, double rho, double p, double vx,
                                           double vy, double vz, double bcx, double bcy, double bcz, double ggas,
                                           double cfl) {
-    const double cs = sqrt((ggas * p) / rho);
-    const double a2 = cs * cs;
-    const double a4 = a2 * a2;
-    const double b2x = (bcx * bcx) / rho;
-    const double b2y = (bcy * bcy) / rho;
-    const double b2z = (bcz * bcz) / rho;
-    const double b2 = (b2x + b2y) + b2z;
-    const double b4 = b2 * b2;
-    const double base = (a4 + (2.0 * a2) * b2) + b4;
-    const double cfx = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2x)));
-    const double cfy = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2y)));
-    const double cfz = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2z)));
-    const double lambda = fmax(fmax(fabs(vx) + cfx, fabs(vy) + cfy), fabs(vz) + cfz);
-    double dxl = T.ax[0].d[j], dyl = T.ax[1].d[k], dzl = T.ax[2].d[l];
-    if (COORD == 2) {
-        dyl = T.ax[0].c[j] * dyl;
-    } else if (COORD == 3) {
-        dyl = T.ax[0].c[j] * dyl;
-        dzl = (T.ax[0].c[j] * T.sinc[k]) * dzl;
-    }
-    return (fmin(fmin(dxl, dyl), dzl) * cfl) / lambda;
+    double dyl = T.ax[1].d[k], dzl = T.ax[2].d[l];
+    if (COORD != 1) cfl_lengths(COORD, T.ax[0].c[j], COORD == 3 ? T.sinc[k] : 0.0, dyl, dzl);
+    return cfl_cell_dt(rho, p, vx, vy, vz, bcx, bcy, bcz, T.ax[0].d[j], dyl, dzl, ggas, cfl);
 }
 
 // block minimum of dt (every thread of the block calls it), then one 64-bit

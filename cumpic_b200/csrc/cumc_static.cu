@@ -11,15 +11,16 @@
 // per-block partial minima of the reduction, in a fixed file-scope device
 // array that exists as soon as the library is loaded.
 //
-// The per-cell formula is the one of finddt (solver/rungekutta.f90:213-247),
-// evaluated in the same order as the library's own finddt kernel, so both give
-// the same double.
+// The per-cell formula is the one of finddt (solver/rungekutta.f90:213-247):
+// cfl_cell_dt and cfl_lengths of cumc_device.cuh, the functions the library's
+// own finddt kernel calls, so both give the same double.
 #include <cuda_runtime.h>
 
 #include <cstdio>
 #include <mutex>
 
 #include "../../include/cumc.h"
+#include "cumc_device.cuh"
 
 namespace {
 
@@ -28,8 +29,8 @@ constexpr int kThreads = 256;
 // active cells (256^3) per call.
 constexpr int kMaxBlocks = CUMC_STATIC_MAX_CELLS / kThreads;
 
-// Scratch shared by every call on a device (128 KiB per device, held until
-// the process exits). No entry needs to start at zero: k_cfl_partial writes
+// Scratch shared by every call on a device (65536 doubles, 512 KiB per
+// device, held until the process exits). No entry needs to start at zero: k_cfl_partial writes
 // partial[0..nblocks) before k_cfl_final reads exactly those entries, on the
 // same stream. Two calls that overlap on the GPU (different streams, no
 // ordering) race on it. Host code must not take this symbol's address
@@ -55,28 +56,11 @@ __global__ void __launch_bounds__(kThreads) k_cfl_partial(int nx, int ny, int nz
         const int k = (int)((t / nx) % ny) + 1;
         const int l = (int)(t / ((long long)nx * ny)) + 1;
         const int i = (j + 2) + SX * ((k + 2) + SY * (l + 2));
-        const double r = rho[i];
-        const double cs = sqrt((ggas * p[i]) / r);
-        const double a2 = cs * cs;
-        const double a4 = a2 * a2;
-        const double b2x = (bcx[i] * bcx[i]) / r;
-        const double b2y = (bcy[i] * bcy[i]) / r;
-        const double b2z = (bcz[i] * bcz[i]) / r;
-        const double b2 = (b2x + b2y) + b2z;
-        const double b4 = b2 * b2;
-        const double base = (a4 + (2.0 * a2) * b2) + b4;
-        const double cfx = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2x)));
-        const double cfy = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2y)));
-        const double cfz = sqrt(0.5 * ((a2 + b2) + sqrt(base - (4.0 * a2) * b2z)));
-        const double lambda = fmax(fmax(fabs(vx[i]) + cfx, fabs(vy[i]) + cfy), fabs(vz[i]) + cfz);
-        double dxl = dxw[j + 3], dyl = dyw[k + 3], dzl = dzw[l + 3];
-        if (coordinate == CUMC_CYLINDRICAL) {
-            dyl = xc[j + 3] * dyl;
-        } else if (coordinate == CUMC_SPHERICAL) {
-            dyl = xc[j + 3] * dyl;
-            dzl = (xc[j + 3] * sinyc[k + 3]) * dzl;
-        }
-        dt_out = (fmin(fmin(dxl, dyl), dzl) * cfl) / lambda;
+        double dyl = dyw[k + 3], dzl = dzw[l + 3];
+        if (coordinate != CUMC_CARTESIAN)
+            cumc::cfl_lengths(coordinate, xc[j + 3], coordinate == CUMC_SPHERICAL ? sinyc[k + 3] : 0.0, dyl, dzl);
+        dt_out = cumc::cfl_cell_dt(rho[i], p[i], vx[i], vy[i], vz[i], bcx[i], bcy[i], bcz[i], dxw[j + 3], dyl, dzl,
+                                   ggas, cfl);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dt_out = fmin(dt_out, __shfl_xor_sync(0xffffffffu, dt_out, o));
@@ -139,6 +123,14 @@ int cumc_cfl_dt_static(int nx, int ny, int nz, const double* rho, const double* 
                        const double* dx, const double* dy, const double* dz, int coordinate, const double* xc,
                        const double* sin_yc, double ggas, double cfl, double* dt_out, void* stream) {
     g_static_error[0] = '\0';
+    // an error left pending by earlier, unrelated work belongs to its caller:
+    // report it without clearing it, and launch nothing
+    cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        snprintf(g_static_error, sizeof g_static_error, "a CUDA error from earlier work is pending (left uncleared): %s",
+                 cudaGetErrorString(pending));
+        return CUMC_ERR_CUDA;
+    }
     if (nx < 1 || ny < 1 || nz < 1) return fail(CUMC_ERR_ARG, "cell counts must be positive");
     const long long cells = (long long)nx * ny * nz;
     if (cells > CUMC_STATIC_MAX_CELLS)

@@ -6,8 +6,8 @@
  * read and write MODULE DEFINITION globals (solver/definition.f90:238-312).
  * This header exports the same steps as plain C functions on an opaque
  * context, so that main.f90 can keep its call sequence through a thin
- * iso_c_binding module and so that C, C++ and Python
- * (ctypes) callers can use the same library.
+ * iso_c_binding module with the subroutines' own names, and so that C, C++
+ * and Python (ctypes) callers can use the same library.
  *
  * Conventions
  *   - Every function returns an int status: CUMC_OK (0) or a CUMC_ERR_* code.
@@ -305,7 +305,7 @@ int cumc_adjoint_run(cumc_ctx* ctx, int nsteps, int checkpoint_every, int object
  * without synchronising.
  *
  * Its only scratch, the per-block partial minima, is a fixed device array of
- * the library (128 KiB per device, held until the process exits), which
+ * the library (512 KiB per device, held until the process exits), which
  * limits a call to CUMC_STATIC_MAX_CELLS active cells; larger grids get
  * CUMC_ERR_LIMIT. The first call on each device looks up that array's device
  * address (cudaGetSymbolAddress), so make a first call on each device before

@@ -4,7 +4,7 @@ the reference's hot-path sources, used only to pin the oracle.
 
 The reference (leon-astrophy/CUMPIC) is Fortran 90 and this image has no
 Fortran compiler. This script reads the reference's own .f90 files where they
-lie (default /root/reference, or $CUMC_REFERENCE), translates the subset of
+lie (the --reference directory; oracle/Makefile passes it), translates the subset of
 Fortran they use (module globals, subroutines and functions with by-reference
 arguments, arrays with explicit lower bounds in column-major order, array
 sections, DO / DO WHILE / IF / SELECT CASE, the intrinsics on the path) into
@@ -33,8 +33,6 @@ import argparse
 import os
 import re
 import sys
-
-REF = os.environ.get("CUMC_REFERENCE", "/root/reference")
 
 SOLVER = ["definition", "setup", "coords", "initial", "rungekutta", "update", "spatial", "reconstruct", "rsolver",
           "flux", "ptou_face", "mhd", "fromrvetou", "ptou", "utop", "boundary"]
@@ -1095,7 +1093,7 @@ static inline int* fai_at(fai* a, int i0, int i1, int i2, int i3) { return a->d 
 """
 
 
-def translate(model: str, ref: str = REF) -> str:
+def translate(model: str, ref: str) -> str:
     units = []
     files = [f"solver/{f}.f90" for f in SOLVER] + MODELS[model]
     # the model's PARAMETER module comes first: definition.f90 does not use it
@@ -1109,7 +1107,7 @@ def translate(model: str, ref: str = REF) -> str:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--model", default="riemann", choices=sorted(MODELS))
-    ap.add_argument("--reference", default=REF)
+    ap.add_argument("--reference", required=True, help="root of the reference's source tree")
     ap.add_argument("-o", "--output", required=True)
     args = ap.parse_args()
     if not os.path.isdir(os.path.join(args.reference, "solver")):

@@ -8,9 +8,11 @@ arrays the caller already owns and keeps its reduction scratch in a fixed
 array inside the library. This test hands it the same state the library's own
 cumc_finddt sees, as device arrays allocated here by the test, and checks that
 both give the same time step, on two calls in a row (the second after one
-RK3 step, so the shared scratch is reused with new contents).
+RK3 step, so the shared scratch is reused with new contents), on a
+Cartesian, a cylindrical and a spherical grid.
 """
 import ctypes
+import math
 
 import numpy as np
 import pytest
@@ -28,6 +30,19 @@ def _widths(f: np.ndarray) -> np.ndarray:
     return d
 
 
+def _centres_and_sines(problem):
+    """cell-centre radius 0.5 (xF(i) + xF(i-1)) and the sine of the polar cell
+    centre, for i = -3..n+3 (index i+3; entry 0 unused), computed with the
+    same double operations and the C library's sin, as the library's own
+    tables are"""
+    xc = np.zeros_like(problem.xf)
+    xc[1:] = 0.5 * (problem.xf[1:] + problem.xf[:-1])
+    sin_yc = np.zeros_like(problem.yf)
+    for i in range(1, len(problem.yf)):
+        sin_yc[i] = math.sin(0.5 * (problem.yf[i] + problem.yf[i - 1]))
+    return xc, sin_yc
+
+
 def _static_dt(sim, problem, torch):
     st = sim.download()
     prim, bcell = st["prim"], st["bcell"]
@@ -35,22 +50,33 @@ def _static_dt(sim, problem, torch):
     fields = [prim[..., q] for q in range(5)] + [bcell[..., q] for q in range(3)]
     arrays = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in fields]
     widths = [torch.from_numpy(_widths(f)).to(dev) for f in (problem.xf, problem.yf, problem.zf)]
+    xc, sin_yc = (torch.from_numpy(a).to(dev) for a in _centres_and_sines(problem))
+    curvilinear = problem.coordinate != N.CARTESIAN
     dt_out = torch.full((1,), -1.0, dtype=torch.float64, device=dev)
     lib = N.lib()
     stream = torch.cuda.current_stream(dev)
     rc = lib.cumc_cfl_dt_static(problem.nx, problem.ny, problem.nz,
                                 *[a.data_ptr() for a in arrays], *[w.data_ptr() for w in widths],
-                                problem.coordinate, None, None, problem.ggas, problem.cfl,
-                                dt_out.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
+                                problem.coordinate, xc.data_ptr() if curvilinear else None,
+                                sin_yc.data_ptr() if problem.coordinate == N.SPHERICAL else None,
+                                problem.ggas, problem.cfl, dt_out.data_ptr(), ctypes.c_void_p(stream.cuda_stream))
     assert rc == N.CUMC_OK, lib.cumc_cfl_dt_static_error()
     stream.synchronize()
     return float(dt_out.item())
 
 
-def test_static_cfl_dt_matches_finddt():
+GRIDS = [
+    ("cartesian", lambda: P.orszag_tang(24, ny=20, nz=16)),
+    ("cylindrical", lambda: P.shell(N.CYLINDRICAL, 16, 12, 10)),
+    ("spherical", lambda: P.torus(24, 16, 8)),
+]
+
+
+@pytest.mark.parametrize("name,make", GRIDS, ids=[g[0] for g in GRIDS])
+def test_static_cfl_dt_matches_finddt(name, make):
     torch = pytest.importorskip("torch")
     from cumpic_b200.solver import CUMC3D
-    problem = P.orszag_tang(24, ny=20, nz=16)
+    problem = make()
     sim = CUMC3D(problem)
     sim.upload()
     sim.initial_update()
