@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--decomp", choices=["replicas", "zslab"], default="replicas",
+                    help="N > 1: independent replicas (weak scaling, the default) or one n^3 box cut into N z-slabs "
+                         "with the halo exchange over NCCL (strong scaling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
@@ -552,11 +555,12 @@ def config_runs(t512: float = 0.05) -> dict:
     return out
 
 
-def adjoint_check(n: int = 128, steps: int = 200, ckpt: int = 20, ndir: int = 16, eps: float = 1e-6) -> dict:
+def adjoint_check(n: int = 128, steps: int = 200, ckpt: int = 20, ndir: int = 8,
+                  eps_list=(1e-5, 1e-6, 1e-7)) -> dict:
     """The adjoint check configuration in full: gradient of the final magnetic
     energy with respect to the initial velocity against central differences
-    (step eps relative to the flow) along `ndir` seeded smooth random
-    directions, with the adjoint's dt sequence replayed."""
+    along `ndir` seeded smooth random directions, at several difference steps
+    (relative to the flow), with the adjoint's dt sequence replayed."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from cumpic_b200 import _native as NN
@@ -577,17 +581,93 @@ def adjoint_check(n: int = 128, steps: int = 200, ckpt: int = 20, ndir: int = 16
             fw.rungekutta(dt)
         return _density(fw.download(), prob, NN.OBJ_MAGNETIC)
 
-    rels = []
-    for dp, _ in smooth_velocity_directions(prob, ndir, 4):
-        fd = float(np.sum(run(prob.prim + eps * dp) - run(prob.prim - eps * dp))) / (2 * eps)
-        ad = float(np.sum(res["grad_prim"] * dp))
-        rels.append(abs(fd - ad) / max(abs(fd), abs(ad)))
-    return {"workload": f"fourier_box n={n} steps={steps} checkpoint_every={ckpt}", "directions": ndir,
-            "eps_relative": eps, "max_rel_err": max(rels), "median_rel_err": statistics.median(rels),
-            "rel_errs": rels}
+    out = {"workload": f"fourier_box n={n} steps={steps} checkpoint_every={ckpt}", "directions": ndir, "by_eps": {}}
+    dirs = list(smooth_velocity_directions(prob, ndir, 4))
+    for eps in eps_list:
+        rels = []
+        for dp, _ in dirs:
+            fd = float(np.sum(run(prob.prim + eps * dp) - run(prob.prim - eps * dp))) / (2 * eps)
+            ad = float(np.sum(res["grad_prim"] * dp))
+            rels.append(abs(fd - ad) / max(abs(fd), abs(ad)))
+        out["by_eps"][f"{eps:g}"] = {"max_rel_err": max(rels), "median_rel_err": statistics.median(rels),
+                                     "rel_errs": rels}
+    best = min(out["by_eps"].values(), key=lambda r: r["median_rel_err"])
+    out["median_rel_err_best_eps"] = best["median_rel_err"]
+    out["max_rel_err_best_eps"] = best["max_rel_err"]
+    return out
 
 
 # ---------------------------------------------------------------------------
+def run_zslab(args, world, rank, local):
+    """One n^3 Orszag-Tang box cut into `world` z-slabs, one per GPU, with the
+    halo exchange over NCCL after every stage (overlapped with the next
+    stage's sweeps of the active planes) and dt the minimum over ranks: K main-
+    loop steps of the whole box, timed on the device, max over ranks
+    (strong scaling)."""
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    from cumpic_b200 import halo
+    from cumpic_b200 import problems as P
+
+    n = args.n
+    prob = P.orszag_tang(n)
+    run = halo.SlabRun(prob, rank, world)
+    run.start()
+    for _ in range(args.warmup):
+        run.step()
+    stream = torch.cuda.ExternalStream(run.sim.stream_handle())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    l0 = run.sim.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        run.step()
+    run.halo.finish()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = run.sim.launch_count() - l0
+    barrier()
+    clk = clocks.stop()
+    ms_max = make_reduce_max(world, "cuda")(ms)
+    value = prob.cells * args.steps / (ms_max / 1e3) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD.format(n=n), "cells": prob.cells, "parallelism": f"zslab x{world}",
+                   "slab_planes": run.slabs.counts,
+                   "l2": "inputs larger than L2 (each of the 8 state arrays is %.2f GB)" % (8 * (n + 6) ** 3 / 1e9)},
+        "gpu_launches": launches, "clocks": clk,
+        "halo": {"bytes_per_face_per_stage": int(11 * 3 * (n + 6) ** 2 * 8),
+                 "transport": "NCCL send/recv on a stream of its own, ordered by CUDA events" if world > 1
+                 else "none (one slab)"},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args, world, rank, local):
     import torch
     import numpy as np
@@ -748,6 +828,8 @@ def main():
     world, rank, local = dist_init()
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.decomp == "zslab":
+        return run_zslab(args, world, rank, local)
     return run_ours(args, world, rank, local)
 
 

@@ -71,11 +71,13 @@ EXPORTS = [
     "cumc_init", "cumc_free", "cumc_last_error", "cumc_upload_state", "cumc_download_state",
     "cumc_initial_update", "cumc_finddt", "cumc_rungekutta", "cumc_spatial", "cumc_download_lrk",
     "cumc_divb", "cumc_advance", "cumc_get_stream", "cumc_profile", "cumc_profile_read",
-    "cumc_launch_count", "cumc_cfl_dt_static", "cumc_cfl_dt_static_error", "cumc_adjoint_run",
+    "cumc_launch_count", "cumc_query", "cumc_cfl_dt_static", "cumc_cfl_dt_static_error", "cumc_adjoint_run",
     "cumc_snapshot_async", "cumc_snapshot_wait", "cumc_restore_state",
-    "cumc_rk_stage", "cumc_halo_doubles", "cumc_halo_pack", "cumc_halo_unpack", "cumc_model_torus",
+    "cumc_rk_stage", "cumc_rk_stage_part", "cumc_halo_doubles", "cumc_halo_pack", "cumc_halo_unpack", "cumc_model_torus",
 ]
 BC_EXCHANGE = -1
+Q_X_STAGING = 1
+Q_FUSED = 2
 STATE_ARRAYS = 17
 
 
@@ -108,12 +110,14 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "cumc_profile": (c_int, [c_void_p, c_int]),
         "cumc_profile_read": (c_int, [c_void_p, c_int, POINTER(c_int), dp]),
         "cumc_launch_count": (c_int, [c_void_p, POINTER(c_longlong)]),
+        "cumc_query": (c_int, [c_void_p, c_int, POINTER(c_longlong)]),
         "cumc_cfl_dt_static": (c_int, [c_int, c_int, c_int] + [c_void_p] * 11 + [c_int, c_void_p, c_void_p,
                                                                                    c_double, c_double, c_void_p,
                                                                                    c_void_p]),
         "cumc_cfl_dt_static_error": (c_char_p, []),
         "cumc_adjoint_run": (c_int, [c_void_p, c_int, c_int, c_int, dp, dp, dp, dp, dp, dp]),
         "cumc_rk_stage": (c_int, [c_void_p, c_int, c_double]),
+        "cumc_rk_stage_part": (c_int, [c_void_p, c_int, c_double, c_int]),
         "cumc_halo_doubles": (c_int, [c_void_p, POINTER(c_longlong)]),
         "cumc_halo_pack": (c_int, [c_void_p, c_int, c_void_p]),
         "cumc_halo_unpack": (c_int, [c_void_p, c_int, c_void_p]),

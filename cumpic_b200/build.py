@@ -58,6 +58,25 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+DRIVER_SRC = os.path.join(HERE, "driver", "cumc_main.c")
+DRIVER = os.path.join(HERE, "driver", "cumc_main")
+# the C caller is plain C99 and must build warning-free against include/cumc.h
+DRIVER_FLAGS = ["-std=c99", "-O2", "-Wall", "-Wextra", "-Werror", "-pedantic"]
+
+
+def build_driver(force: bool = False) -> str:
+    """Compile the C program that drives the library with the reference main
+    program's call sequence (cumpic_b200/driver/cumc_main.c) and link it
+    against libcumc_b200.so."""
+    lib = build_library()
+    if force or _stale(DRIVER, [DRIVER_SRC, lib, os.path.join(ROOT, "include", "cumc.h")]):
+        cmd = ["gcc", *DRIVER_FLAGS, "-o", DRIVER + ".tmp", DRIVER_SRC, "-L" + HERE, "-lcumc_b200",
+               "-Wl,-rpath,$ORIGIN/.."]
+        subprocess.run(cmd, check=True)
+        os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
+
+
 def build_oracle(force: bool = False) -> str:
     """Compile the FP64 CPU oracle (test infrastructure) via oracle/Makefile,
     and, where the reference sources are present, the mechanical translation
@@ -77,4 +96,5 @@ def build_oracle(force: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build_library(force=True, verbose=True))
+    print(build_driver(force=True))
     print(build_oracle())

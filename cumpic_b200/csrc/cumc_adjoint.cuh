@@ -661,20 +661,23 @@ __device__ __forceinline__ void sweep_field(const Prim& pr, const AdjPrim& o, in
 // per (column, field, segment of RC_SEG cells) walks its segment: cell c's
 // reconstruction (vm_out, vp_out) took its seeds from faces c-1 and c; its
 // transpose adds to cells c-2..c+2, kept in a five-cell ring, and a cell is
-// complete once the walk has passed it by two. The four cells next to each
-// end of a segment also receive from the neighbouring segment and are added
-// atomically; the rest with a plain add (no other thread writes them in this
-// launch). The next cell and face seeds are loaded one cell ahead.
+// complete once the walk has passed it by two. A segment writes cells
+// c0-2 .. c1+1, so the four cells next to each end of a segment also receive
+// from the neighbouring segment. The even segments run in one launch and
+// the odd ones in a second (`parity`): within a launch no two threads write
+// the same cell, every add is a plain one, and each cell takes its
+// contributions in a fixed order, so the result is the same bits on every
+// run. The next cell and face seeds are loaded one cell ahead.
 constexpr int RC_SEG = 32;
 
 template <int DIR, int RECON>
-__global__ void __launch_bounds__(128) k_adj_recon_col(Box b, Tabs T, Prim pr, FaceAdj fa, AdjPrim o) {
+__global__ void __launch_bounds__(128) k_adj_recon_col(Box b, Tabs T, Prim pr, FaceAdj fa, AdjPrim o, int parity) {
     using G = WalkGeom<DIR>;
     const long long col = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= G::ncols(b)) return;
     const int v = blockIdx.y;
     const int nd = G::nd(b);
-    const int c0 = blockIdx.z * RC_SEG;
+    const int c0 = (2 * (int)blockIdx.z + parity) * RC_SEG;
     if (c0 > nd + 1) return;
     const int c1 = min(c0 + RC_SEG, nd + 2);  // reconstructed cells 0..nd+1
     const int a = (int)(col % G::wa(b)), cc = (int)(col / G::wa(b));
@@ -688,10 +691,8 @@ __global__ void __launch_bounds__(128) k_adj_recon_col(Box b, Tabs T, Prim pr, F
     dst += base;
     const double* fl = fa.l[v] + base;
     const double* fr = fa.r[v] + base;
-    auto emit = [&](int q, double val, bool shared) {
-        if (val == 0.0) return;
-        if (shared) atomicAdd(dst + q * s, val);
-        else dst[q * s] += val;
+    auto emit = [&](int q, double val) {
+        if (val != 0.0) dst[q * s] += val;
     };
     double x[5] = {src[(c0 - 2) * s], src[(c0 - 1) * s], src[c0 * s], src[(c0 + 1) * s], src[(c0 + 2) * s]};
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // cells c-2..c+2
@@ -702,7 +703,7 @@ __global__ void __launch_bounds__(128) k_adj_recon_col(Box b, Tabs T, Prim pr, F
         const double lvm_n = fr[c * s];  // face c seeds vm_out of cell c+1
         const double lvp_n = c + 1 <= nd ? fl[(c + 1) * s] : 0.0;
         recon_adj<RECON>(A, c, x, lvm, lvp, acc);
-        emit(c - 2, acc[0], c - 2 <= c0 + 1);
+        emit(c - 2, acc[0]);
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             acc[m] = acc[m + 1];
@@ -714,7 +715,7 @@ __global__ void __launch_bounds__(128) k_adj_recon_col(Box b, Tabs T, Prim pr, F
         lvp = lvp_n;
     }
 #pragma unroll
-    for (int m = 0; m < 4; ++m) emit(c1 - 2 + m, acc[m], true);
+    for (int m = 0; m < 4; ++m) emit(c1 - 2 + m, acc[m]);
 }
 
 // sweep^T, pass B along x: the reconstruction transpose with one lane per

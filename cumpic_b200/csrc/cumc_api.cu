@@ -10,7 +10,9 @@
 #include "cumc_mixed.h"
 #include "cumc_walk.cuh"
 #include "cumc_adjoint.cuh"
+#include "cumc_fused.cuh"
 
+#include <cudaTypedefs.h>
 #include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
@@ -52,7 +54,8 @@ struct cumc_ctx {
     double* U[2][8]{};
     double* F[3][7]{};
     double* E[3]{};
-    double* L[8]{};
+    double* L[8]{};      // l_rk (allocated with the FP64 state)
+    bool lrk_valid = false;  // L holds cumc_spatial's l_rk (a fused stage reuses L[0..4] as its accumulator)
     double* staging = nullptr;
     double** dsoa = nullptr;   // device array of 8 pointers for the transposes
     double* scal = nullptr;    // dt, t
@@ -80,8 +83,15 @@ struct cumc_ctx {
     // 4 "walksm" (shared-memory-window walker everywhere), 5 "walkreg"
     // (per-face x, register walker y/z), 6 "xwarp" (lane-per-cell x only;
     // y/z one thread per face), 7 "xface" (per-face x, shared-memory-window
-    // walker y/z)
+    // walker y/z), 8 "fused" (the flux differences fused into the sweeps and
+    // the hydro combine into the z sweep, x rows staged by bulk tensor
+    // copies), 9 "fused_notma" (the same with the x rows loaded directly)
     int sweep_mode = 0;
+    // fused stage (sweep_mode 8): tensor maps of the x sweep's staged fields,
+    // one set per state buffer holding the face fields
+    XaccMaps xmaps[2]{};
+    int xmaps_state = 0;  // 0 not tried, 1 ready, -1 not available (row pitch or driver)
+    const char* xmaps_why = "not tried";
     bool mixed = false;         // CUMC_MIXED: state and kernels of cumc_mixed.cu
     MixedBufs mb{};
     MixedParams mp{};
@@ -89,6 +99,7 @@ struct cumc_ctx {
     void* adj_slab = nullptr;       // adjoint scratch, kept between runs
     size_t adj_slab_bytes = 0;
     int next_stage = 1;    // cumc_rk_stage: the stage due next
+    int part1_stage = 0;   // cumc_rk_stage_part: the stage whose part 1 ran and whose part 2 is due
     bool fuse_dt = false;  // stage 3 also forms the next step's CFL dt (cumc_advance, cumc_rungekutta)
     bool dt_valid = false; // dtmin holds the CFL dt of the current state (set by cumc_rungekutta only)
     int bf_set = 0;        // U[bf_set] holds the current face fields (the last stage's output)
@@ -217,25 +228,34 @@ void launch_grid(cumc_ctx* c, int cls, dim3 grid, int block, size_t smem, K kern
     }
 }
 
+// l_lo, l_cnt: the z planes whose x rows (DIR 0) or y columns (DIR 1) the
+// default kernels sweep (l_cnt < 0: all); the other forms sweep everything
 template <int DIR>
-void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
+void sweep(cumc_ctx* c, const Box& b, const Prim& pr, int l_lo = 0, int l_cnt = -1) {
     FaceFlux out;
     for (int q = 0; q < 7; ++q) out.f[q] = c->F[DIR][q];
     // default: one lane per cell along x, the shared-memory-window walker
     // along y and z
-    const bool walk = (DIR > 0 && (c->sweep_mode == 0 || c->sweep_mode == 5 || c->sweep_mode == 7)) ||
-                      c->sweep_mode == 3 || c->sweep_mode == 4;
+    // modes 0 and 9 come here only for SPATIAL alone (stage 0) and take the
+    // unfused default's kernels
+    const int mode = (c->sweep_mode == 9 || c->sweep_mode == 8) ? 0 : c->sweep_mode;
+    const bool walk = (DIR > 0 && (mode == 0 || mode == 5 || mode == 7)) || mode == 3 || mode == 4;
     if (walk) {  // column walker
         int nseg;
         const int seg = walk_segment(WalkGeom<DIR>::nd(b) + 1, 64, &nseg);
-        const dim3 grid((unsigned)((WalkGeom<DIR>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
+        const int c_cnt = DIR == 1 && l_cnt >= 0 ? l_cnt : WalkGeom<DIR>::wc(b);
+        const int c_lo = DIR == 1 && l_cnt >= 0 ? l_lo : 0;
+        const dim3 grid((unsigned)(((long long)WalkGeom<DIR>::wa(b) * c_cnt + WK_THREADS - 1) / WK_THREADS),
+                        (unsigned)nseg);
         const int cls = CUMC_K_SWEEP_X + DIR;
-        if (c->sweep_mode == 4 || c->sweep_mode == 0 || c->sweep_mode == 7) {
+        if (mode == 4 || mode == 0 || mode == 7) {
             const size_t sm = walk_smem<double>(DIR);
             if (c->recon == CUMC_PPMC)
-                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 4, double>, b, c->tabs, pr, c->ggas, out, seg, out);
+                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 4, double>, b, c->tabs, pr, c->ggas, out,
+                            seg, out, c_lo, c_cnt);
             else
-                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 1, double>, b, c->tabs, pr, c->ggas, out, seg, out);
+                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 1, double>, b, c->tabs, pr, c->ggas, out,
+                            seg, out, c_lo, c_cnt);
         } else {
             const size_t sm = DIR == 0 ? xstage_smem<double>() : 0;
             if (c->recon == CUMC_PPMC)
@@ -245,14 +265,17 @@ void sweep(cumc_ctx* c, const Box& b, const Prim& pr) {
         }
         return;
     }
-    if (DIR == 0 && (c->sweep_mode == 0 || c->sweep_mode == 6)) {  // x: one lane per cell
+    if (DIR == 0 && (mode == 0 || mode == 6)) {  // x: one lane per cell
+        const int cnt = l_cnt >= 0 ? l_cnt : b.nz + 2, lo = l_cnt >= 0 ? l_lo : 0;
         if (c->recon == CUMC_PPMC)
-            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b), 128, k_sweep_xwarp<4, double>, b, c->tabs, pr, c->ggas, out, out);
+            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b, cnt), 128, k_sweep_xwarp<4, double>, b, c->tabs, pr, c->ggas,
+                   out, out, lo, cnt);
         else
-            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b), 128, k_sweep_xwarp<1, double>, b, c->tabs, pr, c->ggas, out, out);
+            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b, cnt), 128, k_sweep_xwarp<1, double>, b, c->tabs, pr, c->ggas,
+                   out, out, lo, cnt);
         return;
     }
-    if (c->sweep_mode != 2) {  // one thread per face
+    if (mode != 2) {  // one thread per face
         const long long n = (long long)((DIR == 0 ? b.nx : b.nx + 1) + 1) * ((DIR == 1 ? b.ny : b.ny + 1) + 1) *
                             ((DIR == 2 ? b.nz : b.nz + 1) + 1);
         if (c->recon == CUMC_PPMC)
@@ -417,11 +440,162 @@ struct NvtxRange {
     ~NvtxRange() { nvtxRangePop(); }
 };
 
-void run_stage(cumc_ctx* c, const Box& b, int stage) {
+// Tensor maps of the x sweep's staged fields (rho, vx, vy, vz, p, by, bz
+// and the face field Bx of either state buffer): 3-D boxes of XA_BOX x
+// XA_ROWS x 1 doubles over the ghosted box, zero fill outside it. A map needs
+// a row pitch that is a multiple of 16 bytes (nx + 6 even); without one, or
+// without the driver entry point, the fused stage loads its rows directly.
+int encode_xmaps(cumc_ctx* c) {
+    const Box& b = c->box;
+    c->xmaps_state = -1;
+    if ((b.SX * sizeof(double)) % 16 != 0) {
+        c->xmaps_why = "row pitch not a multiple of 16 bytes";
+        return CUMC_OK;
+    }
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
+        cudaGetLastError();
+        c->xmaps_why = "no cuTensorMapEncodeTiled entry point";
+        return CUMC_OK;
+    }
+    auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+    const cuuint64_t dims[3] = {(cuuint64_t)b.SX, (cuuint64_t)b.SY, (cuuint64_t)b.SZ};
+    const cuuint64_t strides[2] = {(cuuint64_t)b.SX * sizeof(double), (cuuint64_t)b.SX * b.SY * sizeof(double)};
+    const cuuint32_t box[3] = {XA_BOX, XA_ROWS, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    for (int set = 0; set < 2; ++set) {
+        const double* f[XA_FIELDS] = {c->w[0], c->w[1], c->w[2], c->w[3], c->w[4], c->bc[1], c->bc[2], c->U[set][IBX]};
+        for (int v = 0; v < XA_FIELDS; ++v) {
+            CUresult r = encode(&c->xmaps[set].m[v], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(f[v]), dims,
+                                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) {
+                c->xmaps_why = "cuTensorMapEncodeTiled refused a map";
+                return CUMC_OK;
+            }
+        }
+    }
+    c->xmaps_state = 1;
+    c->xmaps_why = "";
+    return CUMC_OK;
+}
+
+// One RK stage with the flux differences fused into the sweeps and the hydro
+// combine into the z sweep (cumc_fused.cuh): sweeps x, y, z; k_emf; k_ct;
+// k_utop_stage (conversions, and the next CFL dt at stage 3); k_boundary.
+template <int COORD, int RECON>
+void fused_xy(cumc_ctx* c, const Box& b, const Prim& pr, const AccArgs& acc, int fset, int l_lo, int l_cnt) {
+    const bool tma = c->sweep_mode == 8 && c->xmaps_state == 1;
+    const XaccMaps& maps = c->xmaps[fset];
+    if (tma)
+        launch_grid(c, CUMC_K_SWEEP_X, xacc_grid(b, l_cnt), 32 * XA_ROWS, xacc_smem(true),
+                    k_sweep_xacc<RECON, COORD, true>, b, c->tabs, pr, c->ggas, acc, maps, l_lo);
+    else
+        launch_grid(c, CUMC_K_SWEEP_X, xacc_grid(b, l_cnt), 32 * XA_ROWS, xacc_smem(false),
+                    k_sweep_xacc<RECON, COORD, false>, b, c->tabs, pr, c->ggas, acc, maps, l_lo);
+    int nseg;
+    const int seg = walk_segment(WalkGeom<1>::nd(b) + 1, 64, &nseg);
+    const dim3 grid((unsigned)(((long long)WalkGeom<1>::wa(b) * l_cnt + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
+    launch_grid(c, CUMC_K_SWEEP_Y, grid, WK_THREADS, acc_smem<1>(), k_walk_acc<1, RECON, COORD>, b, c->tabs, pr,
+                c->ggas, acc, seg, l_lo, l_cnt);
+}
+
+// x and y sweeps of the planes `part` covers (0: all, 1: the active planes
+// 1..nz, 2: the ghost planes 0 and nz+1), then with part != 1 the z sweep
+template <int COORD, int RECON>
+void fused_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AccArgs& acc, int fset, int part) {
+    if (part == 0) fused_xy<COORD, RECON>(c, b, pr, acc, fset, 0, b.nz + 2);
+    if (part == 1) fused_xy<COORD, RECON>(c, b, pr, acc, fset, 1, b.nz);
+    if (part == 2) {
+        fused_xy<COORD, RECON>(c, b, pr, acc, fset, 0, 1);
+        fused_xy<COORD, RECON>(c, b, pr, acc, fset, b.nz + 1, 1);
+    }
+    if (part == 1) return;
+    int nseg;
+    const int seg = walk_segment(WalkGeom<2>::nd(b) + 1, 64, &nseg);
+    const dim3 grid((unsigned)((WalkGeom<2>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
+    launch_grid(c, CUMC_K_SWEEP_Z, grid, WK_THREADS, acc_smem<2>(), k_walk_acc<2, RECON, COORD>, b, c->tabs, pr,
+                c->ggas, acc, seg, 0, WalkGeom<2>::wc(b));
+}
+
+template <int COORD>
+void fused_tail(cumc_ctx* c, const Box& b, int stage, const CombineArgs& a, const UtopArgs& o) {
+    const long long n = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
+    switch (stage) {
+        case 1: launch(c, CUMC_K_CT, n, 256, k_ct<COORD, 1>, b, c->tabs, a); break;
+        case 2: launch(c, CUMC_K_CT, n, 256, k_ct<COORD, 2>, b, c->tabs, a); break;
+        default: launch(c, CUMC_K_CT, n, 256, k_ct<COORD, 3>, b, c->tabs, a); break;
+    }
+    switch (c->model) {
+        case CUMC_MODEL_NONE: launch(c, CUMC_K_COMBINE, n, 256, k_utop_stage<COORD, 0>, b, c->tabs, o); break;
+        case CUMC_MODEL_RIEMANN: launch(c, CUMC_K_COMBINE, n, 256, k_utop_stage<COORD, 1>, b, c->tabs, o); break;
+        case CUMC_MODEL_TORUS_SPH: launch(c, CUMC_K_COMBINE, n, 256, k_utop_stage<COORD, 2>, b, c->tabs, o); break;
+        default: launch(c, CUMC_K_COMBINE, n, 256, k_utop_stage<COORD, 3>, b, c->tabs, o); break;
+    }
+}
+
+// part 0: the whole stage; part 1: the x and y sweeps of the active planes
+// (they read no ghost plane, so they may run while a halo exchange fills
+// them); part 2: the rest of the stage after part 1
+void fused_stage(cumc_ctx* c, const Box& b, int stage, const Prim& pr, double* const* Un, double* const* Ua,
+                 double* const* dst, int fset, const CombineArgs& a, const UtopArgs& o, int part) {
+    AccArgs acc{};
+    for (int q = 0; q < 5; ++q) {
+        acc.L[q] = c->L[q];
+        acc.u0[q] = Un[q];
+        acc.uc[q] = Ua[q];
+        acc.ud[q] = dst[q];
+        acc.tape[q] = a.tape[q];
+    }
+    for (int d = 0; d < 3; ++d) {
+        acc.fb[d][0] = c->F[d][5];
+        acc.fb[d][1] = c->F[d][6];
+    }
+    acc.dt = c->scal;
+    acc.stage = stage;
+    acc.model = c->model;
+    acc.geom_repeat = c->cfg.geom_source_repeat;
+    acc.rho_floor = c->cfg.rho_floor;
+    acc.r_sh = c->cfg.r_sh;
+    acc.err = c->flag_dev;
+    const bool ppm = c->recon == CUMC_PPMC;
+    switch (c->coord) {
+        case CUMC_CARTESIAN:
+            ppm ? fused_sweeps<1, 4>(c, b, pr, acc, fset, part) : fused_sweeps<1, 1>(c, b, pr, acc, fset, part);
+            break;
+        case CUMC_CYLINDRICAL:
+            ppm ? fused_sweeps<2, 4>(c, b, pr, acc, fset, part) : fused_sweeps<2, 1>(c, b, pr, acc, fset, part);
+            break;
+        default:
+            ppm ? fused_sweeps<3, 4>(c, b, pr, acc, fset, part) : fused_sweeps<3, 1>(c, b, pr, acc, fset, part);
+            break;
+    }
+    if (part == 1) return;
+    FaceFlux ff[3];
+    for (int d = 0; d < 3; ++d)
+        for (int q = 0; q < 7; ++q) ff[d].f[q] = c->F[d][q];
+    EdgeE ee;
+    for (int q = 0; q < 3; ++q) ee.e[q] = c->E[q];
+    launch(c, CUMC_K_EMF, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_emf<double>, b, pr, ff[0], ff[1],
+           ff[2], ee);
+    switch (c->coord) {
+        case CUMC_CARTESIAN: fused_tail<1>(c, b, stage, a, o); break;
+        case CUMC_CYLINDRICAL: fused_tail<2>(c, b, stage, a, o); break;
+        default: fused_tail<3>(c, b, stage, a, o); break;
+    }
+}
+
+// part (fused stages only): 0 the whole stage, 1 the sweeps that read no
+// ghost plane, 2 the rest (see fused_stage); the unfused forms run the whole
+// stage at part 0 and 2 and nothing at part 1
+void run_stage(cumc_ctx* c, const Box& b, int stage, int part = 0) {
+    if (stage > 0) c->lrk_valid = false;
     static const char* const names[4] = {"cumc spatial", "cumc rk stage 1", "cumc rk stage 2", "cumc rk stage 3"};
     const NvtxRange range(names[stage]);
     if (c->mixed) {
-        if (stage > 0)
+        if (stage > 0 && part != 1)
             mixed_stage(mx_launcher(c), b, c->tabs, c->mb, c->mp, stage, stage == 3 && c->fuse_dt ? c->dtmin : nullptr);
         return;
     }
@@ -429,8 +603,43 @@ void run_stage(cumc_ctx* c, const Box& b, int stage) {
     double* const* Ua = c->U[1 - c->cur];
     double* const* src = (stage <= 1) ? Un : Ua;  // arrays holding prim(ibx:ibz) this stage
     const Prim pr = make_prim(c, src);
-    sweep<0>(c, b, pr);
-    sweep<1>(c, b, pr);
+    const bool fused = stage > 0 && !c->mixed && (c->sweep_mode == 8 || c->sweep_mode == 9);
+    const bool split = c->sweep_mode == 0;  // the default kernels take a plane range
+    if (!fused && !split && part == 1) return;
+    if (fused) {
+        CombineArgs a{};
+        double* const* dst = stage == 1 ? Ua : stage == 2 ? Ua : Un;
+        for (int q = 0; q < 8; ++q) {
+            a.u0[q] = Un[q];
+            a.uc[q] = Ua[q];
+            a.ud[q] = dst[q];
+            a.tape[q] = c->tape ? c->tape[(stage - 1) * 8 + q] : nullptr;
+        }
+        a.dt = c->scal;
+        for (int q = 0; q < 3; ++q) a.ecorn[q] = c->E[q];
+        UtopArgs o = utop_args(c, dst, PrimBufs{c->w, c->bc, c->eps});
+        if (stage == 3 && c->fuse_dt) {  // the following iteration's finddt, fused (dtmin reset by the caller)
+            o.dtmin = c->dtmin;
+            o.cfl = c->cfl;
+        }
+        fused_stage(c, b, stage, pr, Un, Ua, dst, src == c->U[0] ? 0 : 1, a, o, part);
+        if (part != 1) boundary(c, b, dst);
+        return;
+    }
+    if (split && part == 1) {  // the x and y sweeps of the active planes: they read no ghost plane
+        sweep<0>(c, b, pr, 1, b.nz);
+        sweep<1>(c, b, pr, 1, b.nz);
+        return;
+    }
+    if (split && part == 2) {  // the rest: the x and y sweeps of the ghost planes 0 and nz+1 first
+        sweep<0>(c, b, pr, 0, 1);
+        sweep<0>(c, b, pr, b.nz + 1, 1);
+        sweep<1>(c, b, pr, 0, 1);
+        sweep<1>(c, b, pr, b.nz + 1, 1);
+    } else {
+        sweep<0>(c, b, pr);
+        sweep<1>(c, b, pr);
+    }
     sweep<2>(c, b, pr);
     FaceFlux ff[3];
     for (int d = 0; d < 3; ++d)
@@ -786,6 +995,8 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
                         : std::strcmp(sw, "walkreg") == 0 ? 5
                         : std::strcmp(sw, "xwarp") == 0   ? 6
                         : std::strcmp(sw, "xface") == 0   ? 7
+                        : std::strcmp(sw, "fused") == 0   ? 8
+                        : std::strcmp(sw, "fused_notma") == 0 ? 9
                                                           : 0;
     }
     if ((rc = sweep_attributes(c)) != CUMC_OK) return fail_init(rc);
@@ -863,6 +1074,8 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
         for (int d = 0; d < 3; ++d)
             for (int q = 0; q < 7; ++q) if ((rc = field(&c->F[d][q])) != CUMC_OK) return fail_init(rc);
         for (int q = 0; q < 3; ++q) if ((rc = field(&c->E[q])) != CUMC_OK) return fail_init(rc);
+        // l_rk: the fused stage's flux-difference accumulator (0-4) and cumc_spatial's output (0-7)
+        for (int q = 0; q < 8; ++q) if ((rc = field(&c->L[q])) != CUMC_OK) return fail_init(rc);
     } else {
         auto ffield = [&](float** p) -> int {
             int r = dalloc(c, p, NT);
@@ -912,6 +1125,9 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
         return fail_init(CUMC_ERR_NOMEM);
     }
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) { cuda_fail(c, e, "init"); return fail_init(CUMC_ERR_CUDA); }
+    if (!c->mixed && c->sweep_mode == 8) encode_xmaps(c);  // before any stream capture: host-side driver calls only
+    if (getenv("CUMC_VERBOSE") && c->sweep_mode == 8 && c->xmaps_state != 1)
+        fprintf(stderr, "cumc: x sweep loads its rows directly: %s\n", c->xmaps_why);
     *out = c;
     return CUMC_OK;
 }
@@ -1055,6 +1271,7 @@ int cumc_finddt(cumc_ctx* c, double* dt) {
     std::memcpy(dt, c->host_pinned, sizeof(double));
     unsigned fl;
     std::memcpy(&fl, c->host_pinned + 1, sizeof(unsigned));
+    if (fl & kTmaTimeoutFlag) return c->fail(CUMC_ERR_CUDA, "a staged bulk tensor copy never completed (wait gave up)");
     if (fl & 1u) return c->fail(CUMC_ERR_NONFINITE, "non-finite density, velocity or pressure in the evolved state");
     return CUMC_OK;
 }
@@ -1076,19 +1293,31 @@ int cumc_rungekutta(cumc_ctx* c, double dt) {
     return sync_status(c);
 }
 
-int cumc_rk_stage(cumc_ctx* c, int stage, double dt) {
+int cumc_rk_stage_part(cumc_ctx* c, int stage, double dt, int part) {
     if (c) c->dt_valid = false;  // the state changes: the cached CFL dt is stale
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
+    if (part < 0 || part > 2) return c->fail(CUMC_ERR_ARG, "part must be 0 (whole stage), 1 or 2");
     if (stage != c->next_stage) return c->fail(CUMC_ERR_STATE, "stage %d called where stage %d is due", stage, c->next_stage);
-    if (stage == 1 && !(dt >= 0.0 && std::isfinite(dt)))
+    if (part == 2 && c->part1_stage != stage)
+        return c->fail(CUMC_ERR_STATE, "part 2 of stage %d called without its part 1", stage);
+    if (part != 2 && c->part1_stage != 0)
+        return c->fail(CUMC_ERR_STATE, "stage %d: part 2 is due", c->part1_stage);
+    if (part != 2 && stage == 1 && !(dt >= 0.0 && std::isfinite(dt)))
         return c->fail(CUMC_ERR_ARG, "dt must be finite and non-negative");
-    if (stage == 1) launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
-    run_stage(c, c->box, stage);
+    if (part != 2 && stage == 1) launch(c, -1, 1, 1, k_set_scalar, c->scal, dt);
+    run_stage(c, c->box, stage, part);
+    if (part == 1) {
+        c->part1_stage = stage;
+        return sync_status(c);
+    }
+    c->part1_stage = 0;
     c->next_stage = stage == 3 ? 1 : stage + 1;
     c->bf_set = stage == 3 ? c->cur : 1 - c->cur;
     return sync_status(c);
 }
+
+int cumc_rk_stage(cumc_ctx* c, int stage, double dt) { return cumc_rk_stage_part(c, stage, dt, 0); }
 
 int cumc_halo_doubles(cumc_ctx* c, long long* n) {
     if (!c || !n) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
@@ -1125,19 +1354,15 @@ int cumc_spatial(cumc_ctx* c) {
     int rc = check_ready(c);
     if (rc != CUMC_OK) return rc;
     if (c->mixed) return c->fail(CUMC_ERR_STATE, "cumc_spatial is available for CUMC_FP64 only");
-    const size_t NT = (size_t)c->box.count();
-    if (!c->L[0])
-        for (int q = 0; q < 8; ++q) {
-            if ((rc = dalloc(c, &c->L[q], NT)) != CUMC_OK) return rc;
-            CUMC_CHECK(cudaMemsetAsync(c->L[q], 0, NT * sizeof(double), c->stream));
-        }
     run_stage(c, c->box, 0);
+    c->lrk_valid = true;
     return sync_status(c);
 }
 
 int cumc_download_lrk(cumc_ctx* c, double* lrk) {
     if (!c || !lrk) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
-    if (!c->L[0]) return c->fail(CUMC_ERR_STATE, "cumc_spatial has not run");
+    if (!c->L[0] || !c->lrk_valid)
+        return c->fail(CUMC_ERR_STATE, "no l_rk to download: cumc_spatial has not run since the last stage");
     const double* s[8] = {c->L[0], c->L[1], c->L[2], c->L[3], c->L[4], c->L[5], c->L[6], c->L[7]};
     return get_soa(c, lrk, 8, s);
 }
@@ -1239,6 +1464,7 @@ int cumc_advance(cumc_ctx* c, int nsteps, double t_end, double* t_inout, int* st
     if (steps_done) *steps_done = st;
     unsigned fl;
     std::memcpy(&fl, c->host_pinned + 2, sizeof(unsigned));
+    if (fl & kTmaTimeoutFlag) return c->fail(CUMC_ERR_CUDA, "a staged bulk tensor copy never completed (wait gave up)");
     if (fl & 1u) return c->fail(CUMC_ERR_NONFINITE, "non-finite density, velocity or pressure in the evolved state");
     return CUMC_OK;
 }
@@ -1273,6 +1499,17 @@ int cumc_profile_read(cumc_ctx* c, int which, int* launches, double* ms) {
     c->prof.clear();
     if (launches) *launches = c->prof_launches[which];
     if (ms) *ms = c->prof_ms[which];
+    return CUMC_OK;
+}
+
+int cumc_query(cumc_ctx* c, int what, long long* value) {
+    if (!c || !value) return c ? c->fail(CUMC_ERR_ARG, "null argument") : CUMC_ERR_ARG;
+    const bool fused = !c->mixed && (c->sweep_mode == 8 || c->sweep_mode == 9);
+    switch (what) {
+        case CUMC_Q_X_STAGING: *value = !fused ? -1 : (c->sweep_mode == 8 && c->xmaps_state == 1) ? 1 : 0; break;
+        case CUMC_Q_FUSED: *value = fused ? 1 : 0; break;
+        default: return c->fail(CUMC_ERR_ARG, "unknown query %d", what);
+    }
     return CUMC_OK;
 }
 
@@ -1368,6 +1605,19 @@ Arr3 arr3(double* const* p) {
     return a;
 }
 
+// reconstruction transpose along y or z: the even segments, then the odd
+// ones (k_adj_recon_col)
+template <int D, int RECON>
+void recon_col(cumc_ctx* c, const Box& b, const Prim& pr, const FaceAdj& fa, const AdjPrim& lp) {
+    const int nseg = (WalkGeom<D>::nd(b) + 2 + RC_SEG - 1) / RC_SEG;
+    for (int parity = 0; parity < 2; ++parity) {
+        const unsigned gz = (unsigned)((nseg - parity + 1) / 2);
+        if (gz == 0) continue;
+        launch_grid(c, -1, dim3((unsigned)((WalkGeom<D>::ncols(b) + 127) / 128), 7, gz), 128, 0,
+                    k_adj_recon_col<D, RECON>, b, c->tabs, pr, fa, lp, parity);
+    }
+}
+
 template <int COORD, int RECON>
 void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, const AdjPrim& lp, double* const* lbf,
                 const FaceAdj& fa) {
@@ -1386,22 +1636,20 @@ void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, c
         const int seg = walk_segment(WalkGeom<D>::nd(b) + 1, 64, &nseg);
         const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
         launch_grid(c, -1, grid, WK_THREADS, walk_smem<double>(D), k_sweep_walk_sm<D, RECON, double, true>, b, c->tabs,
-                    pr, c->ggas, sl, seg, sr);
+                    pr, c->ggas, sl, seg, sr, 0, -1);
     };
     // x: pass A per face, pass B one lane per cell (28 owned cells a warp)
-    launch(c, -1, xwarp_threads(b), 128, k_sweep_xwarp<RECON, double, true>, b, c->tabs, pr, c->ggas, sl, sr);
+    launch(c, -1, xwarp_threads(b), 128, k_sweep_xwarp<RECON, double, true>, b, c->tabs, pr, c->ggas, sl, sr, 0, -1);
     launch(c, -1, fx, 128, k_adj_hll<COORD, 0, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[0]);
     const long long xwarps = (long long)(b.ny + 2) * (b.nz + 2) * ((b.nx + 6 + 27) / 28);
     launch(c, -1, xwarps * 32, 128, k_adj_recon_x<RECON>, b, c->tabs, pr, fa, lp);
     // y, z: pass A per face, pass B one thread per (column, field)
     states(std::integral_constant<int, 1>{});
     launch(c, -1, fy, 128, k_adj_hll<COORD, 1, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[1]);
-    launch_grid(c, -1, dim3((unsigned)((WalkGeom<1>::ncols(b) + 127) / 128), 7, (b.ny + 2 + RC_SEG - 1) / RC_SEG), 128,
-                0, k_adj_recon_col<1, RECON>, b, c->tabs, pr, fa, lp);
+    recon_col<1, RECON>(c, b, pr, fa, lp);
     states(std::integral_constant<int, 2>{});
     launch(c, -1, fz, 128, k_adj_hll<COORD, 2, RECON, true>, b, c->tabs, pr, c->ggas, st, fa, lbf[2]);
-    launch_grid(c, -1, dim3((unsigned)((WalkGeom<2>::ncols(b) + 127) / 128), 7, (b.nz + 2 + RC_SEG - 1) / RC_SEG), 128,
-                0, k_adj_recon_col<2, RECON>, b, c->tabs, pr, fa, lp);
+    recon_col<2, RECON>(c, b, pr, fa, lp);
 }
 
 // boundary^T: gather onto the sources, then clear the ghosts

@@ -211,6 +211,53 @@ struct CombineArgs {
     double rho_floor, r_sh;
 };
 
+// source terms sc of cell (j, k, l) at index i (solver/spatial.f90:75-102:
+// GEOM_SOURCE `geom_repeat` times, then CUSTOM_SOURCE) from the stage's
+// primitives
+template <int COORD, int MODEL>
+__device__ __forceinline__ void cell_sources(const Tabs& T, const Prim& pr, int geom_repeat, double rho_floor,
+                                             double r_sh, int j, int k, int l, int i, double* sc) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) sc[q] = 0.0;
+    if (COORD == 1 && MODEL < 2) return;
+    const double rho = pr.w[0][i], vx = pr.w[1][i], vy = pr.w[2][i], vz = pr.w[3][i], p = pr.w[4][i];
+    const double bx = pr.bc[0][i], by = pr.bc[1][i], bz = pr.bc[2][i];
+    const double x = T.ax[0].c[j];
+    if (COORD == 2) {  // GEOM_SOURCE cylindrical (solver/coords.f90:127-136)
+        const double bsquare = (bx * bx + by * by) + bz * bz;
+        for (int r = 0; r < geom_repeat; ++r) {
+            sc[IVX] = sc[IVX] + (((p + (rho * vy) * vy) + 0.5 * bsquare) - by * by) / (x);
+            sc[IVY] = sc[IVY] - ((rho * vx) * vy - bx * by) / (x);
+        }
+    } else if (COORD == 3) {  // GEOM_SOURCE spherical (solver/coords.f90:139-161)
+        const double bsquare = (bx * bx + by * by) + bz * bz;
+        const double tany = T.tanc[k];
+        for (int r = 0; r < geom_repeat; ++r) {
+            sc[IVX] = sc[IVX] + ((2.0 * p + bx * bx) + rho * (vy * vy + vz * vz)) / (x);
+            sc[IVY] = (sc[IVY] + (((p + (rho * vz) * vz) + 0.5 * bsquare) - bz * bz) / (x * tany)) -
+                      ((rho * vx) * vy - bx * by) / (x);
+            sc[IVZ] = (sc[IVZ] - ((rho * vx) * vz - bx * bz) / (x)) - ((rho * vy) * vz - by * bz) / (x * tany);
+        }
+    }
+    if (MODEL == 2) {  // point-mass gravity (model/torus_sph/src/custom.f90:132-146)
+        const double diff = rho - rho_floor;
+        const double factor = fmax(copysign(1.0, diff), 0.0);
+        const double dphidr = 1.0 / ((x - r_sh) * (x - r_sh));
+        sc[IVX] = sc[IVX] + (((-factor) * rho) * dphidr);
+        sc[ITAU] = sc[ITAU] + ((((-factor) * rho) * vx) * dphidr);
+    } else if (MODEL == 3) {  // gravity in (R, z) (model/torus_cyn/src/custom.f90)
+        const double z = T.ax[2].c[l];
+        const double diff = rho - rho_floor;
+        const double factor = fmax(copysign(1.0, diff), 0.0);
+        const double radius = sqrt(x * x + z * z);
+        const double dphidr = (x / radius) / ((radius - r_sh) * (radius - r_sh));
+        const double dphidz = (z / radius) / ((radius - r_sh) * (radius - r_sh));
+        sc[IVX] = sc[IVX] + (((-factor) * rho) * dphidr);
+        sc[IVZ] = sc[IVZ] + (((-factor) * rho) * dphidz);
+        sc[ITAU] = sc[ITAU] + (((-factor) * rho) * (vx * dphidr + vz * dphidz));
+    }
+}
+
 // hydro l_rk of cell (j, k, l): zero outside the interior
 template <int COORD, int MODEL>
 __device__ __forceinline__ void hydro_lrk(const Tabs& T, const Prim& pr, const FaceFlux& fx, const FaceFlux& fy,
@@ -231,44 +278,8 @@ __device__ __forceinline__ void hydro_lrk(const Tabs& T, const Prim& pr, const F
 #pragma unroll
         for (int q = 0; q < 5; ++q) L[q] = L[q] - (fz.f[q][i] * gp - fz.f[q][i - sl] * gm) / gc;
 
-        // source terms sc (solver/spatial.f90:75-102 and CUSTOM_SOURCE)
-        double sc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        const double rho = pr.w[0][i], vx = pr.w[1][i], vy = pr.w[2][i], vz = pr.w[3][i], p = pr.w[4][i];
-        const double bx = pr.bc[0][i], by = pr.bc[1][i], bz = pr.bc[2][i];
-        const double x = T.ax[0].c[j];
-        if (COORD == 2) {  // GEOM_SOURCE cylindrical (solver/coords.f90:127-136)
-            const double bsquare = (bx * bx + by * by) + bz * bz;
-            for (int r = 0; r < a.geom_repeat; ++r) {
-                sc[IVX] = sc[IVX] + (((p + (rho * vy) * vy) + 0.5 * bsquare) - by * by) / (x);
-                sc[IVY] = sc[IVY] - ((rho * vx) * vy - bx * by) / (x);
-            }
-        } else if (COORD == 3) {  // GEOM_SOURCE spherical (solver/coords.f90:139-161)
-            const double bsquare = (bx * bx + by * by) + bz * bz;
-            const double tany = T.tanc[k];
-            for (int r = 0; r < a.geom_repeat; ++r) {
-                sc[IVX] = sc[IVX] + ((2.0 * p + bx * bx) + rho * (vy * vy + vz * vz)) / (x);
-                sc[IVY] = (sc[IVY] + (((p + (rho * vz) * vz) + 0.5 * bsquare) - bz * bz) / (x * tany)) -
-                          ((rho * vx) * vy - bx * by) / (x);
-                sc[IVZ] = (sc[IVZ] - ((rho * vx) * vz - bx * bz) / (x)) - ((rho * vy) * vz - by * bz) / (x * tany);
-            }
-        }
-        if (MODEL == 2) {  // point-mass gravity (model/torus_sph/src/custom.f90:132-146)
-            const double diff = rho - a.rho_floor;
-            const double factor = fmax(copysign(1.0, diff), 0.0);
-            const double dphidr = 1.0 / ((x - a.r_sh) * (x - a.r_sh));
-            sc[IVX] = sc[IVX] + (((-factor) * rho) * dphidr);
-            sc[ITAU] = sc[ITAU] + ((((-factor) * rho) * vx) * dphidr);
-        } else if (MODEL == 3) {  // gravity in (R, z) (model/torus_cyn/src/custom.f90)
-            const double z = T.ax[2].c[l];
-            const double diff = rho - a.rho_floor;
-            const double factor = fmax(copysign(1.0, diff), 0.0);
-            const double radius = sqrt(x * x + z * z);
-            const double dphidr = (x / radius) / ((radius - a.r_sh) * (radius - a.r_sh));
-            const double dphidz = (z / radius) / ((radius - a.r_sh) * (radius - a.r_sh));
-            sc[IVX] = sc[IVX] + (((-factor) * rho) * dphidr);
-            sc[IVZ] = sc[IVZ] + (((-factor) * rho) * dphidz);
-            sc[ITAU] = sc[ITAU] + (((-factor) * rho) * (vx * dphidr + vz * dphidz));
-        }
+        double sc[5];
+        cell_sources<COORD, MODEL>(T, pr, a.geom_repeat, a.rho_floor, a.r_sh, j, k, l, i, sc);
 #pragma unroll
         for (int q = 0; q < 5; ++q) L[q] = L[q] + sc[q];
     }

@@ -401,14 +401,14 @@ void sweep_mx(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>
         const int seg = walk_segment(WalkGeom<D>::nd(b) + 1, 64, &nseg);
         const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
         const size_t sm = walk_smem<float>(D);
-        if (recon == 4) run(L, DIR, grid, WK_THREADS, sm, k_sweep_walk_sm<D, 4, float>, b, T, pr, ggas, out, seg, out);
-        else run(L, DIR, grid, WK_THREADS, sm, k_sweep_walk_sm<D, 1, float>, b, T, pr, ggas, out, seg, out);
+        if (recon == 4) run(L, DIR, grid, WK_THREADS, sm, k_sweep_walk_sm<D, 4, float>, b, T, pr, ggas, out, seg, out, 0, -1);
+        else run(L, DIR, grid, WK_THREADS, sm, k_sweep_walk_sm<D, 1, float>, b, T, pr, ggas, out, seg, out, 0, -1);
         return;
     }
     // x: one lane per cell
     const long long n = xwarp_threads(b);
-    if (recon == 4) run(L, DIR, g1(n, 128), 128, 0, k_sweep_xwarp<4, float>, b, T, pr, ggas, out, out);
-    else run(L, DIR, g1(n, 128), 128, 0, k_sweep_xwarp<1, float>, b, T, pr, ggas, out, out);
+    if (recon == 4) run(L, DIR, g1(n, 128), 128, 0, k_sweep_xwarp<4, float>, b, T, pr, ggas, out, out, 0, -1);
+    else run(L, DIR, g1(n, 128), 128, 0, k_sweep_xwarp<1, float>, b, T, pr, ggas, out, out, 0, -1);
 }
 
 UtopMx utop_args(const MixedBufs& m, const MixedParams& p) {

@@ -65,7 +65,8 @@ __device__ __forceinline__ int walk_base(const Box& b, long long col) {
 
 // column set-up shared by both window forms. Every thread of a block stays
 // to the end (the x sweep synchronises the block); threads past the last
-// column walk a copy of it and store nothing.
+// column walk a copy of it and store nothing. The columns are those whose
+// slow transverse index lies in c_lo .. c_lo + c_cnt - 1 (c_cnt < 0: all).
 template <int DIR, typename R>
 struct WalkCol {
     int base, s, f0, f1, nd;
@@ -73,17 +74,20 @@ struct WalkCol {
     const R* src[WK_FIELDS];
     int slot[WK_FIELDS];
     const R* bn;
-    __device__ bool init(const Box& b, const PrimT<R>& pr, int seg) {
+    __device__ bool init(const Box& b, const PrimT<R>& pr, int seg, int c_lo = 0, int c_cnt = -1) {
         using G = WalkGeom<DIR>;
         if (b.skip && *b.skip) return false;
+        if (c_cnt < 0) c_cnt = G::wc(b);
+        const long long ncols = (long long)G::wa(b) * c_cnt;
         const long long col = (long long)blockIdx.x * WK_THREADS + threadIdx.x;
-        active = col < G::ncols(b);
+        active = col < ncols;
         nd = G::nd(b);
         f0 = blockIdx.y * seg;
         if (f0 > nd) return false;
         f1 = min(f0 + seg, nd + 1);
         s = G::stride(b);
-        base = walk_base<DIR>(b, col);
+        const long long cc = min(col, ncols - 1);
+        base = G::idx(b, (int)(cc % G::wa(b)), c_lo + (int)(cc / G::wa(b)), 0);
         // tangential cell fields: (by, bz) for x, (bx, bz) for y, (bx, by) for z
         constexpr int ta = DIR == 0 ? 1 : 0;
         constexpr int tb = DIR == 2 ? 1 : 2;
@@ -307,15 +311,16 @@ constexpr size_t walk_smem(int dir) {
 // STATES (y and z only): instead of solving HLL, store each face's
 // reconstructed states, left in out and right in out_r (field order of the
 // sweep, at the face's left cell), for the adjoint's HLL transpose.
+// c_lo, c_cnt: the columns walked (WalkCol; c_cnt < 0 for all)
 template <int DIR, int RECON, typename R, bool STATES = false>
 __global__ void __launch_bounds__(WK_THREADS) k_sweep_walk_sm(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
-                                                             int seg, FaceFluxT<R> out_r) {
+                                                             int seg, FaceFluxT<R> out_r, int c_lo, int c_cnt) {
     static_assert(!STATES || DIR != 0, "face states along y and z");
     extern __shared__ __align__(16) unsigned char wk_raw[];
     R* const sm = reinterpret_cast<R*>(wk_raw) + threadIdx.x;
     auto at = [&](int slot, int v) -> R& { return sm[(slot * WK_FIELDS + v) * WK_THREADS]; };
     WalkCol<DIR, R> C;
-    if (!C.init(b, pr, seg)) return;
+    if (!C.init(b, pr, seg, c_lo, c_cnt)) return;
     const AxisTabs A = T.ax[DIR];
     const int s = C.s, f0 = C.f0;
     XStage<R> X;
@@ -405,18 +410,20 @@ constexpr int XW_FACES = 27;
 
 // STATES: store each face's reconstructed states (left in out, right in
 // out_r, field order of the sweep) instead of solving HLL.
+// The rows are those of the z planes l_lo .. l_lo + l_cnt - 1 (l_cnt < 0: all).
 template <int RECON, typename R, bool STATES = false>
 __global__ void __launch_bounds__(128, 8) k_sweep_xwarp(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
-                                                        FaceFluxT<R> out_r) {
+                                                        FaceFluxT<R> out_r, int l_lo, int l_cnt) {
     constexpr unsigned FULL = 0xffffffffu;
     const int nw = (b.nx + 1 + XW_FACES - 1) / XW_FACES;  // warps per row
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    const long long rows = (long long)(b.ny + 2) * (b.nz + 2);
+    if (l_cnt < 0) l_cnt = b.nz + 2;
+    const long long rows = (long long)(b.ny + 2) * l_cnt;
     if (warp >= rows * nw || (b.skip && *b.skip)) return;  // uniform over the warp
     const int w = (int)(warp % nw);
     const long long row = warp / nw;
-    const int k = (int)(row % (b.ny + 2)), l = (int)(row / (b.ny + 2));
+    const int k = (int)(row % (b.ny + 2)), l = l_lo + (int)(row / (b.ny + 2));
     const int c = w * XW_FACES - 2 + lane;  // this lane's cell; its face is c | c+1
     const bool inb = c >= -2 && c <= b.nx + 3;
     const int ct = min(max(c, -2), b.nx + 3);  // table index kept in range for spare lanes
@@ -462,8 +469,8 @@ __global__ void __launch_bounds__(128, 8) k_sweep_xwarp(Box b, Tabs T, PrimT<R> 
     for (int i = 0; i < 7; ++i) out.f[i][base + c] = fx[i];
 }
 
-inline long long xwarp_threads(const Box& b) {
-    return (long long)(b.ny + 2) * (b.nz + 2) * ((b.nx + 1 + XW_FACES - 1) / XW_FACES) * 32;
+inline long long xwarp_threads(const Box& b, int l_cnt = -1) {
+    return (long long)(b.ny + 2) * (l_cnt < 0 ? b.nz + 2 : l_cnt) * ((b.nx + 1 + XW_FACES - 1) / XW_FACES) * 32;
 }
 
 }  // namespace cumc

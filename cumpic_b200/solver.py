@@ -164,6 +164,11 @@ class CUMC3D:
         at stage 1), for slabs that exchange halos between stages"""
         self._check(self._lib.cumc_rk_stage(self._h, int(stage), float(dt)))
 
+    def rk_stage_part(self, stage: int, dt: float, part: int):
+        """cumc_rk_stage_part: part 1 (the sweeps that read no ghost plane) or
+        part 2 (the rest) of one stage, so a halo exchange can run between"""
+        self._check(self._lib.cumc_rk_stage_part(self._h, int(stage), float(dt), int(part)))
+
     # -- snapshots and restart -------------------------------------------------
     def state_buffer(self) -> np.ndarray:
         """a host buffer for one state (STATE_ARRAYS x shape doubles), pinned
@@ -232,6 +237,12 @@ class CUMC3D:
             self._check(self._lib.cumc_profile_read(self._h, i, ctypes.byref(n), ctypes.byref(ms)))
             out[name] = (n.value, ms.value)
         return out
+
+    def query(self, what: int) -> int:
+        """cumc_query: how the context runs a stage (N.Q_X_STAGING, N.Q_FUSED)"""
+        v = ctypes.c_longlong()
+        self._check(self._lib.cumc_query(self._h, int(what), ctypes.byref(v)))
+        return v.value
 
     def launch_count(self) -> int:
         c = ctypes.c_longlong()

@@ -177,6 +177,19 @@ int cumc_profile_read(cumc_ctx* ctx, int which, int* launches, double* ms);
 /* Number of kernel launches the library issued since cumc_init. */
 int cumc_launch_count(cumc_ctx* ctx, long long* count);
 
+/* Introspection of how the context runs a stage (no counterpart in the
+ * reference). CUMC_Q_FUSED: 1 when the FP64 stages run with the flux
+ * differences fused into the sweeps (environment CUMC_SWEEP=fused or
+ * fused_notma at cumc_init), else 0 (the default: the sweeps write face
+ * fluxes and one kernel combines them). CUMC_Q_X_STAGING: for a fused
+ * context, 1 when its x sweep stages the rows into shared memory by bulk
+ * tensor copies (TMA), 0 when it loads them directly (fused_notma, a row
+ * pitch that is not a multiple of 16 bytes, or no tensor-map support in the
+ * driver); -1 for other contexts. */
+#define CUMC_Q_X_STAGING 1
+#define CUMC_Q_FUSED     2
+int cumc_query(cumc_ctx* ctx, int what, long long* value);
+
 /* Device-side GET_MODEL of the tori (model/torus_sph/src/model.f90:8-284 on
  * a CUMC_SPHERICAL grid, model/torus_cyn/src/model.f90:8-284 on a
  * CUMC_CYLINDRICAL one), for grids too large to build on the host: a
@@ -219,6 +232,16 @@ int cumc_model_torus(cumc_ctx* ctx, const cumc_torus_model* model);
  * (cumc_get_stream). FP64 only. */
 #define CUMC_BC_EXCHANGE (-1)
 int cumc_rk_stage(cumc_ctx* ctx, int stage, double dt);
+/* One RK stage in two parts, so that the halo exchange of the previous
+ * stage's output (the MPI part of the reference's BOUNDARY after each stage,
+ * solver/rungekutta.f90:63,97,141) can run beside the next stage's
+ * computation: part 1 queues the x and y sweeps of the active planes 1..nz,
+ * which read no ghost plane; part 2 queues the rest of the stage and must
+ * follow part 1 of the same stage, after the ghost planes are unpacked.
+ * part 0 is the whole stage (cumc_rk_stage). dt is read at stage 1, part 1
+ * or 0. Forms of the stage without the split (the mixed precision and most
+ * CUMC_SWEEP variants) run everything at part 2. */
+int cumc_rk_stage_part(cumc_ctx* ctx, int stage, double dt, int part);
 int cumc_halo_doubles(cumc_ctx* ctx, long long* n);
 int cumc_halo_pack(cumc_ctx* ctx, int side, double* buf);
 int cumc_halo_unpack(cumc_ctx* ctx, int side, const double* buf);

@@ -1,8 +1,10 @@
-"""z-slab decomposition with the halo exchange (cumc_rk_stage,
+"""z-slab decomposition with the halo exchange (cumc_rk_stage_part,
 cumc_halo_pack/unpack, CUMC_BC_EXCHANGE): a decomposed run equals the
 single-domain run bit for bit (every array, ghosts included), for slabs in
 one process and for two gloo ranks (processes sharing this GPU; the planes
-pass through host memory, and no kernel waits on another process)."""
+pass through host memory, and no kernel waits on another process), and the
+FP64 oracle bit for bit. Each stage's sweeps of the active planes are queued
+before the previous stage's halo is unpacked."""
 import dataclasses
 import os
 import socket
@@ -65,6 +67,43 @@ def test_slabs_in_one_process_match_single_domain(name, make, nslabs):
     _same(run.download(), ref)
 
 
+def test_slabs_match_oracle():
+    """the decomposed run against the FP64 oracle directly (not only against
+    the single-domain CUDA run)"""
+    from _oracle import Oracle
+    from compare import diffs
+    prob = P.orszag_tang(18, ny=14, nz=15)
+    run = halo.LocalSlabs(prob, 3)
+    run.start()
+    o = Oracle(P.orszag_tang(18, ny=14, nz=15), threads=os.cpu_count())
+    o.upload()
+    o.initial_update()
+    for _ in range(4):
+        dt = run.step()
+        assert o.step() == dt
+    d = diffs(run.download(), o.download())
+    assert all(v == 0.0 for v in d.values()), d
+
+
+def test_stage_parts_in_order():
+    from cumpic_b200.solver import CUMC3D
+    s = CUMC3D(halo.ZSlabs(P.orszag_tang(12), 2).local(0))
+    s.upload()
+    s.initial_update()
+    with pytest.raises(N.CumcError) as e:
+        s.rk_stage_part(1, 1e-3, 2)  # part 2 without part 1
+    assert e.value.code == N.CUMC_ERR_STATE
+    s.rk_stage_part(1, 1e-3, 1)
+    with pytest.raises(N.CumcError) as e:
+        s.rk_stage_part(1, 1e-3, 1)  # part 2 is due
+    assert e.value.code == N.CUMC_ERR_STATE
+    with pytest.raises(N.CumcError) as e:
+        s.rk_stage_part(1, 1e-3, 3)
+    assert e.value.code == N.CUMC_ERR_ARG
+    s.rk_stage_part(1, 1e-3, 2)
+    s.rk_stage(2, 0.0)
+
+
 def _rank(rank, world, port, out):
     import torch
     import torch.distributed as dist
@@ -75,7 +114,7 @@ def _rank(rank, world, port, out):
     run.start()
     for _ in range(3):
         run.step()
-    st = run.sim.download()
+    st = run.download()
     np.savez(os.path.join(out, f"r{rank}.npz"), t=run.global_time, **st)
     dist.barrier()
     dist.destroy_process_group()

@@ -202,14 +202,16 @@ def test_nonfinite_state_is_reported(precision):
     assert e.value.code == N.CUMC_ERR_NONFINITE
 
 
-SWEEP_MODES = ["simple", "tile", "walkx", "walksm", "walkreg", "xwarp", "xface"]
+SWEEP_MODES = ["simple", "tile", "walkx", "walksm", "walkreg", "xwarp", "xface", "fused", "fused_notma"]
 
 
 @pytest.mark.parametrize("mode", SWEEP_MODES)
 def test_sweep_variants_bitwise(mode, monkeypatch):
     """Every sweep kernel variant (CUMC_SWEEP, read at cumc_init) gives the
-    default variant's bits; ragged sizes exercise partial blocks, segments
-    and x staging chunks."""
+    default variant's bits, the fused stage (flux differences in the sweeps,
+    x rows staged by TMA) included; ragged sizes exercise partial blocks,
+    segments and x staging chunks, and the odd row pitch of nx = 37 the fused
+    stage's directly loaded x rows."""
     from cumpic_b200.solver import CUMC3D
     out = {}
     for m in (None, mode):
@@ -218,7 +220,8 @@ def test_sweep_variants_bitwise(mode, monkeypatch):
         else:
             monkeypatch.setenv("CUMC_SWEEP", m)
         for name, prob in (("ot", P.orszag_tang(37, ny=29, nz=70)), ("tvd", P.orszag_tang(21, recon=N.TVDMM)),
-                           ("torus", P.torus(24, 16, 8))):
+                           ("torus", P.torus(24, 16, 8)), ("even", P.orszag_tang(58, ny=20, nz=13)),
+                           ("cyl", P.shell(N.CYLINDRICAL, 30, 14, 9))):
             g = CUMC3D(prob)
             g.upload()
             g.initial_update()
@@ -226,6 +229,22 @@ def test_sweep_variants_bitwise(mode, monkeypatch):
                 g.rungekutta(g.finddt())
             out[(m, name)] = g.download()
             g.close()
-    for name in ("ot", "tvd", "torus"):
+    for name in ("ot", "tvd", "torus", "even", "cyl"):
         d = diffs(out[(None, name)], out[(mode, name)])
         assert all(v == 0.0 for v in d.values()), (name, d)
+
+
+def test_fused_stage_stages_x_rows_by_tma(monkeypatch):
+    """CUMC_SWEEP=fused runs the fused sweeps, staging the x rows by bulk
+    tensor copies whenever the row pitch allows (nx + 6 even)"""
+    from cumpic_b200.solver import CUMC3D
+    monkeypatch.delenv("CUMC_SWEEP", raising=False)
+    assert CUMC3D(P.orszag_tang(16)).query(N.Q_FUSED) == 0
+    assert CUMC3D(P.orszag_tang(16)).query(N.Q_X_STAGING) == -1
+    monkeypatch.setenv("CUMC_SWEEP", "fused")
+    assert CUMC3D(P.orszag_tang(16)).query(N.Q_FUSED) == 1
+    assert CUMC3D(P.orszag_tang(16)).query(N.Q_X_STAGING) == 1
+    assert CUMC3D(P.orszag_tang(17)).query(N.Q_X_STAGING) == 0
+    assert CUMC3D(P.orszag_tang(16, precision=N.MIXED)).query(N.Q_FUSED) == 0
+    monkeypatch.setenv("CUMC_SWEEP", "fused_notma")
+    assert CUMC3D(P.orszag_tang(16)).query(N.Q_X_STAGING) == 0
