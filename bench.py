@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-fast", action="store_true", help="skip the CUMC_FP64_FAST section")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-snapshot", action="store_true")
     ap.add_argument("--no-adjoint-check", action="store_true",
@@ -359,9 +360,16 @@ def mixed_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> d
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
+    sim.profile(True)  # per-kernel times of a few more steps (outside the timed region)
+    sim.advance(min(steps, 10))
+    prof = sim.profile_read()
+    sim.profile(False)
     sim.close()
+    tot = max(1e-9, sum(v[1] for v in prof.values()))
     out = {"value": prob.cells * steps / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms / steps,
-           "speedup_vs_fp64": fp64_ms_per_step / (ms / steps), "accuracy_t": prob.t_end, "vs_fp64": {}}
+           "speedup_vs_fp64": fp64_ms_per_step / (ms / steps), "accuracy_t": prob.t_end,
+           "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in prof.items() if v[0]},
+           "kernel_shares": {k: round(v[1] / tot, 4) for k, v in prof.items() if v[0]}, "vs_fp64": {}}
     names = ("rho", "mx", "my", "mz", "E", "bx", "by", "bz")
     for bscale in (1.0, 10.0):
         res = {}
@@ -373,11 +381,69 @@ def mixed_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> d
             res[prec] = (s.download(), s.find_divb()[1], steps_run)
             s.close()
         rel = rel_l1_interior(res[NN.MIXED][0], res[NN.FP64][0])
+        if bscale == 1.0:
+            # the flow's own sensitivity: the FP64 run from a density perturbed by
+            # a seeded 1e-12 relative noise, against the unperturbed FP64 run
+            import numpy as np
+            pp = P.orszag_tang(n, bscale=bscale)
+            rho = pp.prim[..., 0]
+            rho *= 1.0 + 1e-12 * (2.0 * np.random.default_rng(7).random(rho.shape) - 1.0)
+            s = CUMC3D(pp)
+            s.upload()
+            s.initial_update()
+            s.run(pp.t_end)
+            relp = rel_l1_interior(s.download(), res[NN.FP64][0])
+            s.close()
+            out["fp64_perturbed_1e-12_rel_l1_at_t_end"] = {k: relp[q] for q, k in enumerate(names)}
         out["vs_fp64"][f"bscale_{bscale:g}"] = {"rel_l1": {k: rel[q] for q, k in enumerate(names)},
                                                 "max_divb_norm": res[NN.MIXED][1],
                                                 "max_divb_norm_fp64": res[NN.FP64][1],
                                                 "steps": {"fp64": res[NN.FP64][2], "mixed": res[NN.MIXED][2]}}
     return out
+
+
+def fast_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> dict:
+    """CUMC_FP64_FAST (the HLL solve's quotients as products with
+    reciprocals) on the same workload: throughput, its ratio to the bitwise
+    FP64 path, and its relative L1 per conserved variable and normalised
+    max |div B| against the FP64 path (bit-identical to the FP64 oracle) at
+    the configuration's t_end."""
+    import torch
+    from cumpic_b200 import _native as NN
+    from cumpic_b200 import problems as P
+    from cumpic_b200.solver import CUMC3D
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from compare import rel_l1_interior
+
+    prob = P.orszag_tang(n, precision=NN.FP64_FAST)
+    sim = CUMC3D(prob)
+    sim.upload()
+    sim.initial_update()
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    sim.advance(warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.advance(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    sim.close()
+    res = {}
+    for prec in (NN.FP64, NN.FP64_FAST):
+        s = CUMC3D(P.orszag_tang(n, precision=prec))
+        s.upload()
+        s.initial_update()
+        nst = s.run(prob.t_end)
+        res[prec] = (s.download(), s.find_divb()[1], nst)
+        s.close()
+    rel = rel_l1_interior(res[NN.FP64_FAST][0], res[NN.FP64][0])
+    names = ("rho", "mx", "my", "mz", "E", "bx", "by", "bz")
+    return {"value": prob.cells * steps / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms / steps,
+            "speedup_vs_fp64": fp64_ms_per_step / (ms / steps), "accuracy_t": prob.t_end,
+            "steps": {"fp64": res[NN.FP64][2], "fp64_fast": res[NN.FP64_FAST][2]},
+            "rel_l1_vs_fp64": {k: rel[q] for q, k in enumerate(names)},
+            "max_divb_norm": res[NN.FP64_FAST][1]}
 
 
 def snapshot_section(n: int, steps: int = 20) -> dict:
@@ -556,7 +622,7 @@ def config_runs(t512: float = 0.05) -> dict:
 
 
 def adjoint_check(n: int = 128, steps: int = 200, ckpt: int = 20, ndir: int = 8,
-                  eps_list=(1e-5, 1e-6, 1e-7)) -> dict:
+                  eps_list=(1e-6, 1e-7, 1e-8)) -> dict:
     """The adjoint check configuration in full: gradient of the final magnetic
     energy with respect to the initial velocity against central differences
     along `ndir` seeded smooth random directions, at several difference steps
@@ -806,6 +872,8 @@ def run_ours(args, world, rank, local):
     sim.close()
     if world == 1 and not args.no_mixed:
         line["mixed"] = mixed_section(n, args.steps, args.warmup, ms_max / args.steps)
+    if world == 1 and not args.no_fast:
+        line["fp64_fast"] = fast_section(n, args.steps, args.warmup, ms_max / args.steps)
     if world == 1 and not args.no_snapshot:
         line["snapshot"] = snapshot_section(n)
     if world == 1 and not args.no_adjoint:

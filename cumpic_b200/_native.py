@@ -26,7 +26,7 @@ CUMC_ERR_LIMIT = 7
 CARTESIAN, CYLINDRICAL, SPHERICAL = 1, 2, 3
 TVDMM, PPMC = 1, 4
 HLL = 2
-FP64, MIXED = 0, 1
+FP64, MIXED, FP64_FAST = 0, 1, 2
 MODEL_NONE, MODEL_RIEMANN, MODEL_TORUS_SPH, MODEL_TORUS_CYN = 0, 1, 2, 3
 
 OBJ_MAGNETIC, OBJ_KINETIC, OBJ_LINEAR = 1, 2, 3

@@ -93,6 +93,7 @@ struct cumc_ctx {
     int xmaps_state = 0;  // 0 not tried, 1 ready, -1 not available (row pitch or driver)
     const char* xmaps_why = "not tried";
     bool mixed = false;         // CUMC_MIXED: state and kernels of cumc_mixed.cu
+    bool fast = false;          // CUMC_FP64_FAST: the default sweeps' HLL with reciprocal products
     MixedBufs mb{};
     MixedParams mp{};
     double* const* tape = nullptr;  // adjoint: 3 x 8 arrays receiving each stage's combine output
@@ -250,12 +251,15 @@ void sweep(cumc_ctx* c, const Box& b, const Prim& pr, int l_lo = 0, int l_cnt = 
         const int cls = CUMC_K_SWEEP_X + DIR;
         if (mode == 4 || mode == 0 || mode == 7) {
             const size_t sm = walk_smem<double>(DIR);
-            if (c->recon == CUMC_PPMC)
-                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 4, double>, b, c->tabs, pr, c->ggas, out,
-                            seg, out, c_lo, c_cnt);
+            const bool ppm = c->recon == CUMC_PPMC;
+            if (c->fast)
+                launch_grid(c, cls, grid, WK_THREADS, sm,
+                            ppm ? k_sweep_walk_sm<DIR, 4, double, false, true> : k_sweep_walk_sm<DIR, 1, double, false, true>,
+                            b, c->tabs, pr, c->ggas, out, seg, out, c_lo, c_cnt);
             else
-                launch_grid(c, cls, grid, WK_THREADS, sm, k_sweep_walk_sm<DIR, 1, double>, b, c->tabs, pr, c->ggas, out,
-                            seg, out, c_lo, c_cnt);
+                launch_grid(c, cls, grid, WK_THREADS, sm,
+                            ppm ? k_sweep_walk_sm<DIR, 4, double> : k_sweep_walk_sm<DIR, 1, double>, b, c->tabs, pr,
+                            c->ggas, out, seg, out, c_lo, c_cnt);
         } else {
             const size_t sm = DIR == 0 ? xstage_smem<double>() : 0;
             if (c->recon == CUMC_PPMC)
@@ -267,12 +271,15 @@ void sweep(cumc_ctx* c, const Box& b, const Prim& pr, int l_lo = 0, int l_cnt = 
     }
     if (DIR == 0 && (mode == 0 || mode == 6)) {  // x: one lane per cell
         const int cnt = l_cnt >= 0 ? l_cnt : b.nz + 2, lo = l_cnt >= 0 ? l_lo : 0;
-        if (c->recon == CUMC_PPMC)
-            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b, cnt), 128, k_sweep_xwarp<4, double>, b, c->tabs, pr, c->ggas,
-                   out, out, lo, cnt);
+        const bool ppm = c->recon == CUMC_PPMC;
+        if (c->fast)
+            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b, cnt), 128,
+                   ppm ? k_sweep_xwarp<4, double, false, true> : k_sweep_xwarp<1, double, false, true>, b, c->tabs, pr,
+                   c->ggas, out, out, lo, cnt);
         else
-            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b, cnt), 128, k_sweep_xwarp<1, double>, b, c->tabs, pr, c->ggas,
-                   out, out, lo, cnt);
+            launch(c, CUMC_K_SWEEP_X, xwarp_threads(b, cnt), 128,
+                   ppm ? k_sweep_xwarp<4, double> : k_sweep_xwarp<1, double>, b, c->tabs, pr, c->ggas, out, out, lo,
+                   cnt);
         return;
     }
     if (mode != 2) {  // one thread per face
@@ -914,15 +921,16 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     if (cfg->coordinate < 1 || cfg->coordinate > 3) return bad("coordinate must be 1 (cartesian), 2 (cylindrical) or 3 (spherical)");
     if (cfg->recon != CUMC_PPMC && cfg->recon != CUMC_TVDMM) return bad("recon must be CUMC_PPMC or CUMC_TVDMM (the reference implements no other)");
     if (cfg->solver != CUMC_HLL) return bad("solver must be CUMC_HLL (the reference implements no other)");
-    if (cfg->precision != CUMC_FP64 && cfg->precision != CUMC_MIXED) return bad("precision must be CUMC_FP64 or CUMC_MIXED");
+    if (cfg->precision != CUMC_FP64 && cfg->precision != CUMC_MIXED && cfg->precision != CUMC_FP64_FAST)
+        return bad("precision must be CUMC_FP64, CUMC_FP64_FAST or CUMC_MIXED");
     if (cfg->model < 0 || cfg->model > 3) return bad("unknown model id");
     for (int i = 0; i < 6; ++i)
         if ((cfg->boundary_flag[i] < 0 || cfg->boundary_flag[i] > 4) &&
             !(i >= 4 && cfg->boundary_flag[i] == CUMC_BC_EXCHANGE))
             return bad("boundary_flag entries must be 0..4 (z faces: or CUMC_BC_EXCHANGE)");
     if ((cfg->boundary_flag[4] == CUMC_BC_EXCHANGE || cfg->boundary_flag[5] == CUMC_BC_EXCHANGE) &&
-        cfg->precision != CUMC_FP64)
-        return bad("CUMC_BC_EXCHANGE faces need CUMC_FP64");
+        cfg->precision == CUMC_MIXED)
+        return bad("CUMC_BC_EXCHANGE faces need CUMC_FP64 or CUMC_FP64_FAST");
     if (cfg->boundary_flag[0] == 4 || cfg->boundary_flag[1] == 4)
         return bad("equatorial symmetry is not allowed for the x-boundary (solver/setup.f90:147-151)");
     if (cfg->boundary_flag[4] == 3 || cfg->boundary_flag[5] == 3)
@@ -1001,6 +1009,7 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     }
     if ((rc = sweep_attributes(c)) != CUMC_OK) return fail_init(rc);
     c->mixed = cfg->precision == CUMC_MIXED;
+    c->fast = cfg->precision == CUMC_FP64_FAST;
     if (c->mixed && (e = mixed_attributes()) != cudaSuccess) {
         cuda_fail(c, e, "cudaFuncSetAttribute(mixed sweep smem)");
         return fail_init(CUMC_ERR_CUDA);
@@ -1888,7 +1897,7 @@ extern "C" int cumc_adjoint_run(cumc_ctx* c, int nsteps, int checkpoint_every, i
     if (c) c->dt_valid = false;
     if (!c) return CUMC_ERR_ARG;
     if (!c->uploaded) return c->fail(CUMC_ERR_STATE, "cumc_upload_state must come first");
-    if (c->mixed || c->exchange || (c->model != CUMC_MODEL_NONE && c->model != CUMC_MODEL_RIEMANN))
+    if (c->mixed || c->fast || c->exchange || (c->model != CUMC_MODEL_NONE && c->model != CUMC_MODEL_RIEMANN))
         return c->fail(CUMC_ERR_CONFIG, "the adjoint covers CUMC_FP64 with model NONE or RIEMANN on one domain");
     if (nsteps < 1 || checkpoint_every < 1) return c->fail(CUMC_ERR_ARG, "nsteps and checkpoint_every must be >= 1");
     if (objective < CUMC_OBJ_MAGNETIC || objective > CUMC_OBJ_LINEAR) return c->fail(CUMC_ERR_ARG, "unknown objective");

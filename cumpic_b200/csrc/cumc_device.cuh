@@ -129,6 +129,20 @@ __device__ __forceinline__ R signalspeed(R cs, R bn, R bt1, R bt2, R rho) {
     return sqrt(R(0.5) * ((a2 + b2) + sqrt(fmax(((a4 + b4) + (R(2) * b2) * a2) - (R(4) * a2) * b2n, R(0)))));
 }
 
+// compute_signalspeed with the quotients by rho formed as products with
+// irho = 1/rho (the CUMC_FP64_FAST form: not bit-compatible with the reference)
+template <typename R>
+__device__ __forceinline__ R signalspeed_recip(R cs, R bn, R bt1, R bt2, R irho) {
+    const R a2 = cs * cs;
+    const R a4 = a2 * a2;
+    const R b2n = (bn * bn) * irho;
+    const R b2t1 = (bt1 * bt1) * irho;
+    const R b2t2 = (bt2 * bt2) * irho;
+    const R b2 = (b2n + b2t1) + b2t2;
+    const R b4 = b2 * b2;
+    return sqrt(R(0.5) * ((a2 + b2) + sqrt(fmax(((a4 + b4) + (R(2) * b2) * a2) - (R(4) * a2) * b2n, R(0)))));
+}
+
 // compute_roe (solver/definition.f90:387-392)
 template <typename R>
 __device__ __forceinline__ R roe_avg(R xl, R xr, R sl, R sr) {
@@ -152,12 +166,15 @@ template <int DIR, typename R>
 struct FaceSide {
     static constexpr int t1 = (DIR + 1) % 3, t2 = (DIR + 2) % 3;
     R rho, v[3], p, b[3], E, hb2, vdotb;
-    __device__ __forceinline__ FaceSide(const R w[8], R ggas) {
+    struct GivenEps {};
+    __device__ __forceinline__ FaceSide(const R w[8], R ggas)
+        : FaceSide(w, (w[ITAU] / w[IRHO]) / (ggas - R(1)), GivenEps{}) {}
+    // e: the side's specific internal energy, EOS_EPSILON (model/riemann/src/eos.f90:194)
+    __device__ __forceinline__ FaceSide(const R w[8], R e, GivenEps) {
         rho = w[IRHO];
         v[0] = w[IVX]; v[1] = w[IVY]; v[2] = w[IVZ];
         p = w[ITAU];
         b[0] = w[IBX]; b[1] = w[IBY]; b[2] = w[IBZ];
-        const R e = (p / rho) / (ggas - R(1));  // EOS_EPSILON (model/riemann/src/eos.f90:194)
         const R vsquare = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
         const R bsquare = (b[0] * b[0] + b[1] * b[1]) + b[2] * b[2];
         E = rho * (e + R(0.5) * vsquare) + R(0.5) * bsquare;
@@ -184,21 +201,46 @@ struct FaceSide {
 // HLL flux at a face from the left and right primitive states (8 each,
 // natural order). out receives the 7 stored components: rho, rho v, E and
 // the two tangential fields in natural (x, y, z) order.
-template <int DIR, typename R>
+//
+// RECIP (the CUMC_FP64_FAST form, not bit-compatible with the reference):
+// the 21 quotients of a face share five divisors (rho of either side,
+// ggas - 1, the Roe weight sum, sR - sL), so each divisor's reciprocal is
+// formed once and the quotients become products; the values differ from the
+// reference's by a few units in the last place.
+template <int DIR, typename R, bool RECIP = false>
 __device__ __forceinline__ void hll_flux7(const R wl[8], const R wr[8], R ggas, R out[7]) {
     constexpr int ivn = IVX + DIR;
     constexpr int ibn = IBX + DIR, ibt1 = IBX + (DIR + 1) % 3, ibt2 = IBX + (DIR + 2) % 3;
-    const FaceSide<DIR, R> L(wl, ggas), Rs(wr, ggas);
-    // EOS_SOUNDSPEED (model/riemann/src/eos.f90:168)
-    const R csL = sqrt((ggas * wl[ITAU]) / wl[IRHO]);
-    const R csR = sqrt((ggas * wr[ITAU]) / wr[IRHO]);
-    const R cfsL = signalspeed(csL, wl[ibn], wl[ibt1], wl[ibt2], wl[IRHO]);
-    const R cfsR = signalspeed(csR, wr[ibn], wr[ibt1], wr[ibt2], wr[IRHO]);
-    const R sqL = sqrt(wl[IRHO]), sqR = sqrt(wr[IRHO]);
-    const R ubar = roe_avg(wl[ivn], wr[ivn], sqL, sqR);
-    const R cbar = roe_avg(cfsL, cfsR, sqL, sqR);
-    const R sL = fmin(wl[ivn] - cfsL, ubar - cbar);
-    const R sR = fmax(wr[ivn] + cfsR, ubar + cbar);
+    using Side = FaceSide<DIR, R>;
+    R sL, sR;
+    Side L = RECIP ? Side(wl, wl[ITAU] * (R(1) / wl[IRHO]) * (R(1) / (ggas - R(1))), typename Side::GivenEps{})
+                   : Side(wl, ggas);
+    Side Rs = RECIP ? Side(wr, wr[ITAU] * (R(1) / wr[IRHO]) * (R(1) / (ggas - R(1))), typename Side::GivenEps{})
+                    : Side(wr, ggas);
+    if (RECIP) {
+        const R irL = R(1) / wl[IRHO], irR = R(1) / wr[IRHO];
+        const R csL = sqrt((ggas * wl[ITAU]) * irL);
+        const R csR = sqrt((ggas * wr[ITAU]) * irR);
+        const R cfsL = signalspeed_recip(csL, wl[ibn], wl[ibt1], wl[ibt2], irL);
+        const R cfsR = signalspeed_recip(csR, wr[ibn], wr[ibt1], wr[ibt2], irR);
+        const R sqL = sqrt(wl[IRHO]), sqR = sqrt(wr[IRHO]);
+        const R isq = R(1) / (sqL + sqR);
+        const R ubar = (sqL * wl[ivn] + sqR * wr[ivn]) * isq;
+        const R cbar = (sqL * cfsL + sqR * cfsR) * isq;
+        sL = fmin(wl[ivn] - cfsL, ubar - cbar);
+        sR = fmax(wr[ivn] + cfsR, ubar + cbar);
+    } else {
+        // EOS_SOUNDSPEED (model/riemann/src/eos.f90:168)
+        const R csL = sqrt((ggas * wl[ITAU]) / wl[IRHO]);
+        const R csR = sqrt((ggas * wr[ITAU]) / wr[IRHO]);
+        const R cfsL = signalspeed(csL, wl[ibn], wl[ibt1], wl[ibt2], wl[IRHO]);
+        const R cfsR = signalspeed(csR, wr[ibn], wr[ibt1], wr[ibt2], wr[IRHO]);
+        const R sqL = sqrt(wl[IRHO]), sqR = sqrt(wr[IRHO]);
+        const R ubar = roe_avg(wl[ivn], wr[ivn], sqL, sqR);
+        const R cbar = roe_avg(cfsL, cfsR, sqL, sqR);
+        sL = fmin(wl[ivn] - cfsL, ubar - cbar);
+        sR = fmax(wr[ivn] + cfsR, ubar + cbar);
+    }
     constexpr int bt_a = DIR == 0 ? IBY : IBX;  // stored tangential components
     constexpr int bt_b = DIR == 2 ? IBY : IBZ;
     const int comp[7] = {IRHO, IVX, IVY, IVZ, ITAU, bt_a, bt_b};
@@ -206,8 +248,18 @@ __device__ __forceinline__ void hll_flux7(const R wl[8], const R wr[8], R ggas, 
 #pragma unroll
         for (int c = 0; c < 7; ++c) out[c] = L.f(comp[c]);
     } else if (sL <= R(0) && sR >= R(0)) {
+        if (RECIP) {
+            const R ids = R(1) / (sR - sL);
 #pragma unroll
-        for (int c = 0; c < 7; ++c) out[c] = fluxhll(L.f(comp[c]), Rs.f(comp[c]), L.u(comp[c]), Rs.u(comp[c]), sL, sR);
+            for (int c = 0; c < 7; ++c) {
+                const R yl = L.f(comp[c]), yr = Rs.f(comp[c]), xl = L.u(comp[c]), xr = Rs.u(comp[c]);
+                out[c] = ((sR * yl - sL * yr) + (sL * sR) * (xr - xl)) * ids;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 7; ++c)
+                out[c] = fluxhll(L.f(comp[c]), Rs.f(comp[c]), L.u(comp[c]), Rs.u(comp[c]), sL, sR);
+        }
     } else {
 #pragma unroll
         for (int c = 0; c < 7; ++c) out[c] = Rs.f(comp[c]);

@@ -214,13 +214,13 @@ __device__ __forceinline__ void walk_step(const AxisTabs& A, int f, R v0, R v1, 
 }
 
 // HLL at face f; the x sweep parks the fluxes in the staging slots (j)
-template <int DIR, typename R>
+template <int DIR, typename R, bool RECIP = false>
 __device__ __forceinline__ void walk_flux(const WalkCol<DIR, R>& C, int f, R (&wl)[8], R (&wr)[8], R ggas,
                                           FaceFluxT<R>& out, R bn, XStage<R>& X, int j) {
     wl[IBX + DIR] = bn;
     wr[IBX + DIR] = bn;
     R fx[7];
-    hll_flux7<DIR>(wl, wr, ggas, fx);
+    hll_flux7<DIR, R, RECIP>(wl, wr, ggas, fx);
     if (DIR == 0) {
 #pragma unroll
         for (int i = 0; i < 7; ++i) X.put(i, j, fx[i]);
@@ -312,7 +312,8 @@ constexpr size_t walk_smem(int dir) {
 // reconstructed states, left in out and right in out_r (field order of the
 // sweep, at the face's left cell), for the adjoint's HLL transpose.
 // c_lo, c_cnt: the columns walked (WalkCol; c_cnt < 0 for all)
-template <int DIR, int RECON, typename R, bool STATES = false>
+// RECIP: the HLL solve's quotients as products with reciprocals (hll_flux7)
+template <int DIR, int RECON, typename R, bool STATES = false, bool RECIP = false>
 __global__ void __launch_bounds__(WK_THREADS) k_sweep_walk_sm(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
                                                              int seg, FaceFluxT<R> out_r, int c_lo, int c_cnt) {
     static_assert(!STATES || DIR != 0, "face states along y and z");
@@ -383,7 +384,7 @@ __global__ void __launch_bounds__(WK_THREADS) k_sweep_walk_sm(Box b, Tabs T, Pri
                 }
             }
         } else {
-            walk_flux<DIR>(C, f, wl, wr, ggas, out, bn, X, j);
+            walk_flux<DIR, R, RECIP>(C, f, wl, wr, ggas, out, bn, X, j);
         }
     }
     if (DIR == 0) walk_last(C, X, out);
@@ -411,7 +412,7 @@ constexpr int XW_FACES = 27;
 // STATES: store each face's reconstructed states (left in out, right in
 // out_r, field order of the sweep) instead of solving HLL.
 // The rows are those of the z planes l_lo .. l_lo + l_cnt - 1 (l_cnt < 0: all).
-template <int RECON, typename R, bool STATES = false>
+template <int RECON, typename R, bool STATES = false, bool RECIP = false>
 __global__ void __launch_bounds__(128, 8) k_sweep_xwarp(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
                                                         FaceFluxT<R> out_r, int l_lo, int l_cnt) {
     constexpr unsigned FULL = 0xffffffffu;
@@ -464,7 +465,7 @@ __global__ void __launch_bounds__(128, 8) k_sweep_xwarp(Box b, Tabs T, PrimT<R> 
     wl[IBX] = bn;
     wr[IBX] = bn;
     R fx[7];
-    hll_flux7<0>(wl, wr, ggas, fx);
+    hll_flux7<0, R, RECIP>(wl, wr, ggas, fx);
 #pragma unroll
     for (int i = 0; i < 7; ++i) out.f[i][base + c] = fx[i];
 }

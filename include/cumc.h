@@ -57,6 +57,10 @@ extern "C" {
 
 /* arithmetic of the path */
 #define CUMC_FP64  0  /* all FP64, bit-compatible with the FP64 restatement  */
+#define CUMC_FP64_FAST 2  /* FP64 throughout, but the HLL solve forms its 21
+                            quotients a face as products with 5 reciprocals:
+                            not bit-compatible, within a few ulp a face
+                            (no counterpart in the reference)                */
 #define CUMC_MIXED 1  /* FP32 reconstruction/HLL/EMF, compensated FP32 state,
                          FP64 energy and pressure recovery                   */
 
@@ -82,7 +86,7 @@ typedef struct cumc_config {
     double cfl;              /* Courant number (solver/definition.f90:116)        */
     int recon;               /* CUMC_PPMC or CUMC_TVDMM                            */
     int solver;              /* CUMC_HLL                                           */
-    int precision;           /* CUMC_FP64 or CUMC_MIXED                            */
+    int precision;           /* CUMC_FP64, CUMC_FP64_FAST or CUMC_MIXED            */
     int model;               /* CUMC_MODEL_*                                       */
     double rho_floor;        /* torus models: atmosphere density floor            */
     double eps_floor;        /* torus models: specific internal energy floor      */
