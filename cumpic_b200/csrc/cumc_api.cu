@@ -11,6 +11,7 @@
 #include "cumc_walk.cuh"
 #include "cumc_adjoint.cuh"
 #include "cumc_fused.cuh"
+#include "cumc_emfct.cuh"
 
 #include <cudaTypedefs.h>
 #include <nvtx3/nvToolsExt.h>
@@ -44,6 +45,7 @@ struct cumc_ctx {
     signed char fac[6][8]{};
     std::string err;
     int device = 0;
+    int sm_count = 148;  // multiprocessors of the device (grid sizing)
     cudaStream_t stream = nullptr;
 
     std::vector<void*> allocs;
@@ -94,6 +96,9 @@ struct cumc_ctx {
     const char* xmaps_why = "not tried";
     bool mixed = false;         // CUMC_MIXED: state and kernels of cumc_mixed.cu
     bool fast = false;          // CUMC_FP64_FAST: the default sweeps' HLL with reciprocal products
+    // the edge EMFs and the CT update in one tiled kernel (k_emf_ct) instead of
+    // k_emf + k_ct; environment CUMC_EMF=pair selects the pair (A/B timing)
+    bool emf_tiles = true;
     MixedBufs mb{};
     MixedParams mp{};
     double* const* tape = nullptr;  // adjoint: 3 x 8 arrays receiving each stage's combine output
@@ -243,9 +248,9 @@ void sweep(cumc_ctx* c, const Box& b, const Prim& pr, int l_lo = 0, int l_cnt = 
     const bool walk = (DIR > 0 && (mode == 0 || mode == 5 || mode == 7)) || mode == 3 || mode == 4;
     if (walk) {  // column walker
         int nseg;
-        const int seg = walk_segment(WalkGeom<DIR>::nd(b) + 1, 64, &nseg);
         const int c_cnt = DIR == 1 && l_cnt >= 0 ? l_cnt : WalkGeom<DIR>::wc(b);
         const int c_lo = DIR == 1 && l_cnt >= 0 ? l_lo : 0;
+        const int seg = walk_segment_for<DIR>(b, (long long)WalkGeom<DIR>::wa(b) * c_cnt, c->sm_count, &nseg);
         const dim3 grid((unsigned)(((long long)WalkGeom<DIR>::wa(b) * c_cnt + WK_THREADS - 1) / WK_THREADS),
                         (unsigned)nseg);
         const int cls = CUMC_K_SWEEP_X + DIR;
@@ -328,7 +333,11 @@ void combine_stage(cumc_ctx* c, const Box& b, const Prim& pr, const FaceFlux* ff
         return;
     }
     constexpr int S = STAGE == 0 ? 1 : STAGE;
-    launch(c, CUMC_K_CT, n, 256, k_ct<COORD, S>, b, c->tabs, a);
+    if (c->emf_tiles)
+        launch_grid(c, CUMC_K_CT, emf_ct_grid(b), EC_TX * EC_TY, sizeof(EmfCtSmem), k_emf_ct<COORD, S>, b, c->tabs, pr,
+                    ff[0], ff[1], ff[2], a);
+    else
+        launch(c, CUMC_K_CT, n, 256, k_ct<COORD, S>, b, c->tabs, a);
     launch(c, CUMC_K_COMBINE, n, 256, k_combine_utop<COORD, MODEL, S>, b, c->tabs, pr, ff[0], ff[1], ff[2], a, o);
 }
 
@@ -503,7 +512,7 @@ void fused_xy(cumc_ctx* c, const Box& b, const Prim& pr, const AccArgs& acc, int
         launch_grid(c, CUMC_K_SWEEP_X, xacc_grid(b, l_cnt), 32 * XA_ROWS, xacc_smem(false),
                     k_sweep_xacc<RECON, COORD, false>, b, c->tabs, pr, c->ggas, acc, maps, l_lo);
     int nseg;
-    const int seg = walk_segment(WalkGeom<1>::nd(b) + 1, 64, &nseg);
+    const int seg = walk_segment_for<1>(b, (long long)WalkGeom<1>::wa(b) * l_cnt, c->sm_count, &nseg);
     const dim3 grid((unsigned)(((long long)WalkGeom<1>::wa(b) * l_cnt + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
     launch_grid(c, CUMC_K_SWEEP_Y, grid, WK_THREADS, acc_smem<1>(), k_walk_acc<1, RECON, COORD>, b, c->tabs, pr,
                 c->ggas, acc, seg, l_lo, l_cnt);
@@ -521,7 +530,7 @@ void fused_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AccArgs& acc,
     }
     if (part == 1) return;
     int nseg;
-    const int seg = walk_segment(WalkGeom<2>::nd(b) + 1, 64, &nseg);
+    const int seg = walk_segment_for<2>(b, WalkGeom<2>::ncols(b), c->sm_count, &nseg);
     const dim3 grid((unsigned)((WalkGeom<2>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
     launch_grid(c, CUMC_K_SWEEP_Z, grid, WK_THREADS, acc_smem<2>(), k_walk_acc<2, RECON, COORD>, b, c->tabs, pr,
                 c->ggas, acc, seg, 0, WalkGeom<2>::wc(b));
@@ -653,7 +662,11 @@ void run_stage(cumc_ctx* c, const Box& b, int stage, int part = 0) {
         for (int q = 0; q < 7; ++q) ff[d].f[q] = c->F[d][q];
     EdgeE ee;
     for (int q = 0; q < 3; ++q) ee.e[q] = c->E[q];
-    launch(c, CUMC_K_EMF, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_emf<double>, b, pr, ff[0], ff[1], ff[2], ee);
+    // the edge EMFs: k_emf here and k_ct in the combine, or (the default
+    // stages) both in k_emf_ct there
+    if (stage == 0 || !c->emf_tiles)
+        launch(c, CUMC_K_EMF, (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256, k_emf<double>, b, pr, ff[0], ff[1],
+               ff[2], ee);
 
     CombineArgs a{};
     double* const* dst = stage == 1 ? Ua : stage == 2 ? Ua : Un;
@@ -993,6 +1006,10 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     };
     int rc;
     if ((e = cudaGetDevice(&c->device)) != cudaSuccess) { cuda_fail(c, e, "cudaGetDevice"); return fail_init(CUMC_ERR_CUDA); }
+    if ((e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device)) != cudaSuccess) {
+        cuda_fail(c, e, "cudaDeviceGetAttribute");
+        return fail_init(CUMC_ERR_CUDA);
+    }
     {
         const char* sw = getenv("CUMC_SWEEP");
         c->sweep_mode = !sw                              ? 0
@@ -1006,6 +1023,10 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
                         : std::strcmp(sw, "fused") == 0   ? 8
                         : std::strcmp(sw, "fused_notma") == 0 ? 9
                                                           : 0;
+    }
+    {
+        const char* em = getenv("CUMC_EMF");
+        c->emf_tiles = !(em && std::strcmp(em, "pair") == 0);
     }
     if ((rc = sweep_attributes(c)) != CUMC_OK) return fail_init(rc);
     c->mixed = cfg->precision == CUMC_MIXED;
@@ -1118,6 +1139,7 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
         mp.coord = c->coord;
         mp.recon = c->recon;
         mp.geom_repeat = c->cfg.geom_source_repeat;
+        mp.sm_count = c->sm_count;
     }
     if ((rc = dalloc(c, &c->dsoa, 8)) != CUMC_OK) return fail_init(rc);
     if ((rc = dalloc(c, &c->scal, 4)) != CUMC_OK) return fail_init(rc);
@@ -1642,7 +1664,7 @@ void adj_sweeps(cumc_ctx* c, const Box& b, const Prim& pr, const AdjStage& st, c
     auto states = [&](auto dir) {
         constexpr int D = decltype(dir)::value;
         int nseg;
-        const int seg = walk_segment(WalkGeom<D>::nd(b) + 1, 64, &nseg);
+        const int seg = walk_segment_for<D>(b, WalkGeom<D>::ncols(b), c->sm_count, &nseg);
         const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
         launch_grid(c, -1, grid, WK_THREADS, walk_smem<double>(D), k_sweep_walk_sm<D, RECON, double, true>, b, c->tabs,
                     pr, c->ggas, sl, seg, sr, 0, -1);

@@ -1,0 +1,149 @@
+// cumc_emfct.cuh — edge EMFs and the constrained-transport update of the
+// face fields in one kernel (the EMF sums of GET_FLUXES,
+// solver/spatial.f90:190-203,268-281,346-359, flux_ct's ecell/ecorn,
+// solver/mhd.f90:95-125, its curl, :130-153, and the RK combine of the face
+// fields, solver/rungekutta.f90:41-51,75-85,109-119).
+//
+// k_emf writes the three edge-EMF arrays and k_ct reads them back at six
+// neighbouring edges a face triple. Here a block owns a tile of 32 x 8 face
+// triples (x fastest) and marches in z over a segment of planes. Per plane
+// it forms, in shared memory, the cell EMFs E = -v x B of the cells the
+// plane's edges average, then the edge EMFs of the tile and of the halo row
+// and column its CT reads (Ez at j-1 and k-1; Ey at j-1; Ex at k-1), and
+// keeps the x and y edge EMFs of the previous plane (the l-1 edges of CT).
+// Each cell EMF is formed once per plane, each edge EMF at most 1.2 times.
+// Edges with an index of -1 are zero, as the never-written entries of the
+// edge arrays are for k_ct. Every value is the same expression, in the same
+// order, as in k_emf and k_ct, so the result is bit for bit theirs.
+#pragma once
+#include "cumc_kernels.cuh"
+
+namespace cumc {
+
+constexpr int EC_TX = 32, EC_TY = 8;           // face triples of a tile
+constexpr int EC_CX = EC_TX + 2, EC_CY = EC_TY + 2;  // cells j0-1..j0+32, k0-1..k0+8
+constexpr int EC_EX = EC_TX + 1, EC_EY = EC_TY + 1;  // edges j0-1..j0+31, k0-1..k0+7
+constexpr int EC_SEG = 32;                     // planes a block marches over
+
+struct EmfCtSmem {
+    double ec[2][3][EC_CY][EC_CX];   // cell EMFs of two planes (ring by plane parity)
+    double ex[2][EC_EY][EC_EX];      // x edge EMFs of two planes (ring by plane parity)
+    double ey[2][EC_EY][EC_EX];      // y edge EMFs of two planes
+    double ez[EC_EY][EC_EX];         // z edge EMFs of the current plane
+};
+
+// cell EMFs of plane l for the tile's cells (zero outside -1..n+1)
+__device__ __forceinline__ void ec_cells(const Box& b, const Prim& pr, EmfCtSmem& S, int j0, int k0, int l) {
+    const int slot = l & 1;
+    for (int t = threadIdx.x; t < EC_CX * EC_CY; t += EC_TX * EC_TY) {
+        const int cj = t % EC_CX, ck = t / EC_CX;
+        const int j = j0 - 1 + cj, k = k0 - 1 + ck;
+        double x = 0.0, y = 0.0, z = 0.0;
+        if (j <= b.nx + 1 && k <= b.ny + 1 && l >= -1 && l <= b.nz + 1) {
+            const int i = b.idx(j, k, l);
+            x = ecell_x(pr, i);
+            y = ecell_y(pr, i);
+            z = ecell_z(pr, i);
+        }
+        S.ec[slot][0][ck][cj] = x;
+        S.ec[slot][1][ck][cj] = y;
+        S.ec[slot][2][ck][cj] = z;
+    }
+}
+
+// edge EMFs of plane l (x and y edges into their ring slot; z edges with `z`)
+__device__ __forceinline__ void ec_edges(const Box& b, const FaceFlux& fx, const FaceFlux& fy, const FaceFlux& fz,
+                                         EmfCtSmem& S, int j0, int k0, int l, bool z) {
+    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
+    const double q = 0.25;
+    const int c0 = l & 1, c1 = (l + 1) & 1;  // cell-EMF slots of planes l and l+1
+    const int e = l & 1;
+    for (int t = threadIdx.x; t < EC_EX * EC_EY; t += EC_TX * EC_TY) {
+        const int ej = t % EC_EX, ek = t / EC_EX;  // edge (j0 - 1 + ej, k0 - 1 + ek)
+        const int j = j0 - 1 + ej, k = k0 - 1 + ek;
+        const bool live = j >= 0 && k >= 0 && l >= 0 && j <= b.nx && k <= b.ny && l <= b.nz;
+        const int i = live ? b.idx(j, k, l) : 0;
+        // cell (j, k) of the edge is cell slot (ck, cj) = (ek, ej): the edge sits
+        // at the upper faces of cells j and k
+        const int cj = ej, ck = ek;
+        double ex = 0.0, ey = 0.0, ez = 0.0;
+        if (live) {
+            ex = 0.0 + q * (-fy.f[6][i] - fy.f[6][i + sl]);
+            ex = ex + q * (fz.f[6][i] + fz.f[6][i + sk]);
+            ey = 0.0 + q * (fx.f[6][i] + fx.f[6][i + sl]);
+            ey = ey + q * (-fz.f[5][i] - fz.f[5][i + sj]);
+            // k_emf's sums: cells (j,k,l), (j,k,l+1), (j,k+1,l), (j,k+1,l+1) for Ex;
+            // (j,k,l), (j,k,l+1), (j+1,k,l), (j+1,k,l+1) for Ey; (j,k), (j,k+1),
+            // (j+1,k), (j+1,k+1) of plane l for Ez
+            ex = ex * 2.0 - q * (((S.ec[c0][0][ck][cj] + S.ec[c1][0][ck][cj]) + S.ec[c0][0][ck + 1][cj]) +
+                                 S.ec[c1][0][ck + 1][cj]);
+            ey = ey * 2.0 - q * (((S.ec[c0][1][ck][cj] + S.ec[c1][1][ck][cj]) + S.ec[c0][1][ck][cj + 1]) +
+                                 S.ec[c1][1][ck][cj + 1]);
+            if (z) {
+                ez = 0.0 + q * (-fx.f[5][i] - fx.f[5][i + sk]);
+                ez = ez + q * (fy.f[5][i] + fy.f[5][i + sj]);
+                ez = ez * 2.0 - q * (((S.ec[c0][2][ck][cj] + S.ec[c0][2][ck + 1][cj]) + S.ec[c0][2][ck][cj + 1]) +
+                                     S.ec[c0][2][ck + 1][cj + 1]);
+            }
+        }
+        S.ex[e][ek][ej] = ex;
+        S.ey[e][ek][ej] = ey;
+        if (z) S.ez[ek][ej] = ez;
+    }
+}
+
+template <int COORD, int STAGE>
+__global__ void __launch_bounds__(EC_TX * EC_TY, 6) k_emf_ct(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy,
+                                                          FaceFlux fz, CombineArgs a) {
+    extern __shared__ __align__(16) unsigned char ec_raw[];
+    EmfCtSmem& S = *reinterpret_cast<EmfCtSmem*>(ec_raw);
+    if (b.skip && *b.skip) return;
+    const int j0 = blockIdx.x * EC_TX, k0 = blockIdx.y * EC_TY;
+    const int l0 = blockIdx.z * EC_SEG, l1 = min(l0 + EC_SEG, b.nz + 1);
+    const int tj = threadIdx.x % EC_TX, tk = threadIdx.x / EC_TX;
+    const int j = j0 + tj, k = k0 + tk;
+    const bool mine = j <= b.nx && k <= b.ny;
+    const double dt = *a.dt;
+
+    // prologue: the x and y edges of plane l0 - 1 (zero for l0 = 0)
+    ec_cells(b, pr, S, j0, k0, l0 - 1);
+    ec_cells(b, pr, S, j0, k0, l0);
+    __syncthreads();
+    ec_edges(b, fx, fy, fz, S, j0, k0, l0 - 1, false);
+    __syncthreads();
+    for (int l = l0; l < l1; ++l) {
+        ec_cells(b, pr, S, j0, k0, l + 1);  // replaces plane l - 1's cells
+        __syncthreads();
+        ec_edges(b, fx, fy, fz, S, j0, k0, l, true);
+        __syncthreads();
+        if (mine) {
+            // ct_lrk (solver/mhd.f90:137-148) on the shared-memory edges; the tile's
+            // (tj, tk) is edge (tj + 1, tk + 1)
+            const int ej = tj + 1, ek = tk + 1, e = l & 1, em = (l - 1) & 1;
+            const double Ez = S.ez[ek][ej], Ez_km = S.ez[ek - 1][ej], Ez_jm = S.ez[ek][ej - 1];
+            const double Ey = S.ey[e][ek][ej], Ey_lm = S.ey[em][ek][ej], Ey_jm = S.ey[e][ek][ej - 1];
+            const double Ex = S.ex[e][ek][ej], Ex_lm = S.ex[em][ek][ej], Ex_km = S.ex[e][ek - 1][ej];
+            CTf g;
+            geom_ct<COORD>(T, j, k, l, g);
+            double L[3];
+            L[0] = -((Ez * g.bx_ez_p - Ez_km * g.bx_ez_m) / g.bx_ez_c - (Ey * g.bx_ey_p - Ey_lm * g.bx_ey_m) / g.bx_ey_c);
+            L[1] = -((Ex * g.by_ex_p - Ex_lm * g.by_ex_m) / g.by_ex_c - (Ez * g.by_ez_p - Ez_jm * g.by_ez_m) / g.by_ez_c);
+            L[2] = -((Ey * g.bz_ey_p - Ey_jm * g.bz_ey_m) / g.bz_ey_c - (Ex * g.bz_ex_p - Ex_km * g.bz_ex_m) / g.bz_ex_c);
+            const int i = b.idx(j, k, l);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double r = rk_point<STAGE>(a.u0[IBX + c][i], STAGE == 1 ? 0.0 : a.uc[IBX + c][i], dt, L[c]);
+                a.ud[IBX + c][i] = r;
+                if (a.tape[IBX + c]) a.tape[IBX + c][i] = r;
+            }
+        }
+        __syncthreads();  // the next plane overwrites the z edges and a cell-EMF slot
+    }
+}
+
+inline dim3 emf_ct_grid(const Box& b) {
+    return dim3((unsigned)((b.nx + 1 + EC_TX - 1) / EC_TX), (unsigned)((b.ny + 1 + EC_TY - 1) / EC_TY),
+                (unsigned)((b.nz + 1 + EC_SEG - 1) / EC_SEG));
+}
+
+}  // namespace cumc

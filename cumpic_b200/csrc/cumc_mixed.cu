@@ -392,13 +392,13 @@ __global__ void __launch_bounds__(256) k_export_mx(Box b, UtopMx a, double* __re
 
 template <int DIR>
 void sweep_mx(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>& pr, float ggas, const MixedBufs& m,
-              int recon) {
+              int recon, int sm_count) {
     FaceFluxT<float> out;
     for (int q = 0; q < 7; ++q) out.f[q] = m.F[DIR][q];
     if (DIR > 0) {  // column walker along y or z, window in shared memory
         constexpr int D = DIR > 0 ? DIR : 1;
         int nseg;
-        const int seg = walk_segment(WalkGeom<D>::nd(b) + 1, 64, &nseg);
+        const int seg = walk_segment_for<D>(b, WalkGeom<D>::ncols(b), sm_count, &nseg);
         const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
         const size_t sm = walk_smem<float>(D);
         if (recon == 4) run(L, DIR, grid, WK_THREADS, sm, k_sweep_walk_sm<D, 4, float>, b, T, pr, ggas, out, seg, out, 0, -1);
@@ -496,9 +496,9 @@ void mixed_stage(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs
     for (int q = 0; q < 5; ++q) pr.w[q] = m.w[q];
     for (int q = 0; q < 3; ++q) { pr.bc[q] = m.bc[q]; pr.bf[q] = m.bf[q]; }
     const float ggas = (float)p.ggas;
-    sweep_mx<0>(L, b, T, pr, ggas, m, p.recon);
-    sweep_mx<1>(L, b, T, pr, ggas, m, p.recon);
-    sweep_mx<2>(L, b, T, pr, ggas, m, p.recon);
+    sweep_mx<0>(L, b, T, pr, ggas, m, p.recon, p.sm_count);
+    sweep_mx<1>(L, b, T, pr, ggas, m, p.recon, p.sm_count);
+    sweep_mx<2>(L, b, T, pr, ggas, m, p.recon, p.sm_count);
     FaceFluxT<float> ff[3];
     for (int d = 0; d < 3; ++d)
         for (int q = 0; q < 7; ++q) ff[d].f[q] = m.F[d][q];

@@ -38,6 +38,7 @@ struct MixedParams {
     int eps_yout;
     signed char fac[6][8];
     int model, coord, recon, geom_repeat;
+    int sm_count;  // multiprocessors of the device (grid sizing)
 };
 
 // How the mixed kernels are launched: the caller's stream, and hooks that

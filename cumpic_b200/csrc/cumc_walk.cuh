@@ -54,6 +54,21 @@ inline int walk_segment(int faces, int target, int* nseg) {
     return (faces + n - 1) / n;
 }
 
+// segments of a walk along DIR over `ncols` columns: about 64 faces each,
+// shorter (down to 8) while the grid would give fewer than 32 warps per SM,
+// so that small boxes (a 128^3 adjoint box, the torus) still fill the GPU.
+// Each segment repeats the walk's prologue (three slopes, two interface
+// values, one fix a field), a few per cent of a face's work at 8 faces.
+template <int DIR>
+inline int walk_segment_for(const Box& b, long long ncols, int sm_count, int* nseg) {
+    const int faces = WalkGeom<DIR>::nd(b) + 1;
+    const long long blocks = (ncols + WK_THREADS - 1) / WK_THREADS;
+    const long long want = (long long)sm_count * 32 / (WK_THREADS / 32);  // blocks for 32 warps per SM
+    int target = 64;
+    while (target > 8 && blocks * ((faces + target - 1) / target) < want) target /= 2;
+    return walk_segment(faces, target, nseg);
+}
+
 // cell index 0 (along DIR) of column `col` of the block's grid, clamped to
 // the last column so that the spare threads of the last block stay in bounds
 template <int DIR>

@@ -248,3 +248,28 @@ def test_fused_stage_stages_x_rows_by_tma(monkeypatch):
     assert CUMC3D(P.orszag_tang(16, precision=N.MIXED)).query(N.Q_FUSED) == 0
     monkeypatch.setenv("CUMC_SWEEP", "fused_notma")
     assert CUMC3D(P.orszag_tang(16)).query(N.Q_X_STAGING) == 0
+
+
+def test_emf_ct_tiles_equal_the_pair(monkeypatch):
+    """the tiled EMF + CT kernel (default) gives the bits of k_emf + k_ct
+    (CUMC_EMF=pair) on Cartesian, cylindrical and spherical grids, ragged
+    tiles and short z segments included"""
+    from cumpic_b200.solver import CUMC3D
+    out = {}
+    for mode in (None, "pair"):
+        if mode:
+            monkeypatch.setenv("CUMC_EMF", mode)
+        else:
+            monkeypatch.delenv("CUMC_EMF", raising=False)
+        for name, prob in (("ot", P.orszag_tang(37, ny=29, nz=70)), ("cyl", P.shell(N.CYLINDRICAL, 30, 14, 9)),
+                           ("torus", P.torus(24, 16, 8))):
+            g = CUMC3D(prob)
+            g.upload()
+            g.initial_update()
+            for _ in range(2):
+                g.rungekutta(g.finddt())
+            out[(mode, name)] = g.download()
+            g.close()
+    for name in ("ot", "cyl", "torus"):
+        d = diffs(out[(None, name)], out[("pair", name)])
+        assert all(v == 0.0 for v in d.values()), (name, d)
