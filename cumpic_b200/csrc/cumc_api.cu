@@ -99,6 +99,10 @@ struct cumc_ctx {
     // the edge EMFs and the CT update in one tiled kernel (k_emf_ct) instead of
     // k_emf + k_ct; environment CUMC_EMF=pair selects the pair (A/B timing)
     bool emf_tiles = true;
+    // the hydro combine on cell pairs (k_combine_utop2) when the row stride is
+    // even and the arrays are 16-byte aligned; CUMC_COMBINE=scalar selects
+    // k_combine_utop (A/B timing)
+    bool pair_combine = true;
     MixedBufs mb{};
     MixedParams mp{};
     double* const* tape = nullptr;  // adjoint: 3 x 8 arrays receiving each stage's combine output
@@ -323,6 +327,22 @@ struct PrimBufs {
 
 UtopArgs utop_args(cumc_ctx* c, double* const* u, const PrimBufs& p);
 
+// k_combine_utop2's conditions: an even row stride and 16-byte alignment of
+// every array it reads or writes as pairs
+inline bool al16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+template <int STAGE>
+bool pairs_aligned(const Box& b, const FaceFlux* ff, const CombineArgs& a, const UtopArgs& o) {
+    if (b.SX & 1) return false;
+    bool ok = al16(o.eps);
+    for (int q = 0; q < 5; ++q) {
+        ok = ok && al16(ff[0].f[q]) && al16(ff[1].f[q]) && al16(ff[2].f[q]) && al16(a.u0[q]) && al16(o.u[q]) &&
+             al16(o.w[q]) && (!a.tape[q] || al16(a.tape[q]));
+        if (STAGE != 1) ok = ok && al16(a.uc[q]);
+    }
+    for (int q = 0; q < 3; ++q) ok = ok && al16(o.u[IBX + q]) && al16(o.bc[q]);
+    return ok;
+}
+
 // stage 0: l_rk alone; stages 1-3: face fields, then hydro combine + conversions
 template <int COORD, int MODEL, int STAGE>
 void combine_stage(cumc_ctx* c, const Box& b, const Prim& pr, const FaceFlux* ff, const CombineArgs& a,
@@ -338,7 +358,13 @@ void combine_stage(cumc_ctx* c, const Box& b, const Prim& pr, const FaceFlux* ff
                     ff[0], ff[1], ff[2], a);
     else
         launch(c, CUMC_K_CT, n, 256, k_ct<COORD, S>, b, c->tabs, a);
-    launch(c, CUMC_K_COMBINE, n, 256, k_combine_utop<COORD, MODEL, S>, b, c->tabs, pr, ff[0], ff[1], ff[2], a, o);
+    if (c->pair_combine && pairs_aligned<S>(b, ff, a, o)) {
+        const long long np = (long long)((b.nx + 2) / 2) * (b.ny + 1) * (b.nz + 1);
+        launch(c, CUMC_K_COMBINE, np, 256, k_combine_utop2<COORD, MODEL, S>, b, c->tabs, pr, ff[0], ff[1], ff[2], a,
+               o);
+    } else {
+        launch(c, CUMC_K_COMBINE, n, 256, k_combine_utop<COORD, MODEL, S>, b, c->tabs, pr, ff[0], ff[1], ff[2], a, o);
+    }
 }
 
 template <int COORD, int MODEL>
@@ -1027,6 +1053,8 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
     {
         const char* em = getenv("CUMC_EMF");
         c->emf_tiles = !(em && std::strcmp(em, "pair") == 0);
+        const char* cm = getenv("CUMC_COMBINE");
+        c->pair_combine = !(cm && std::strcmp(cm, "scalar") == 0);
     }
     if ((rc = sweep_attributes(c)) != CUMC_OK) return fail_init(rc);
     c->mixed = cfg->precision == CUMC_MIXED;

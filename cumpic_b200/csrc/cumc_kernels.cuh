@@ -258,7 +258,15 @@ __device__ __forceinline__ void cell_sources(const Tabs& T, const Prim& pr, int 
     }
 }
 
-// hydro l_rk of cell (j, k, l): zero outside the interior
+// one direction's share of a cell's hydro l_rk: the flux difference of the
+// faces above (fp) and below (fm) with the geometry factors of GEOM_FLUX
+// (solver/spatial.f90:171-187)
+__device__ __forceinline__ double flux_diff(double L, double fp, double fm, double gp, double gm, double gc) {
+    return L - (fp * gp - fm * gm) / gc;
+}
+
+// hydro l_rk of cell (j, k, l): zero outside the interior; inside, the x, y, z
+// flux differences in that order, then the sources (solver/spatial.f90:365-375)
 template <int COORD, int MODEL>
 __device__ __forceinline__ void hydro_lrk(const Tabs& T, const Prim& pr, const FaceFlux& fx, const FaceFlux& fy,
                                           const FaceFlux& fz, const CombineArgs& a, int j, int k, int l, int i,
@@ -270,13 +278,13 @@ __device__ __forceinline__ void hydro_lrk(const Tabs& T, const Prim& pr, const F
         double gp, gc, gm;
         geom_flux<COORD, 0>(T, j, k, l, gp, gc, gm);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) L[q] = L[q] - (fx.f[q][i] * gp - fx.f[q][i - sj] * gm) / gc;
+        for (int q = 0; q < 5; ++q) L[q] = flux_diff(L[q], fx.f[q][i], fx.f[q][i - sj], gp, gm, gc);
         geom_flux<COORD, 1>(T, j, k, l, gp, gc, gm);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) L[q] = L[q] - (fy.f[q][i] * gp - fy.f[q][i - sk] * gm) / gc;
+        for (int q = 0; q < 5; ++q) L[q] = flux_diff(L[q], fy.f[q][i], fy.f[q][i - sk], gp, gm, gc);
         geom_flux<COORD, 2>(T, j, k, l, gp, gc, gm);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) L[q] = L[q] - (fz.f[q][i] * gp - fz.f[q][i - sl] * gm) / gc;
+        for (int q = 0; q < 5; ++q) L[q] = flux_diff(L[q], fz.f[q][i], fz.f[q][i - sl], gp, gm, gc);
 
         double sc[5];
         cell_sources<COORD, MODEL>(T, pr, a.geom_repeat, a.rho_floor, a.r_sh, j, k, l, i, sc);
@@ -285,7 +293,6 @@ __device__ __forceinline__ void hydro_lrk(const Tabs& T, const Prim& pr, const F
     }
 }
 
-// field l_rk of face triple (j, k, l): the CT update (solver/mhd.f90:137-148)
 template <int COORD>
 __device__ __forceinline__ void ct_lrk(const Tabs& T, const double* const* ecorn, int j, int k, int l, int i, int sk,
                                        int sl, double* L) {
@@ -396,10 +403,20 @@ __device__ __forceinline__ void bcell_point(const Box& b, const UtopArgs& a, int
     }
 }
 
-// the conversions of one cell; with FROM_CONS the hydro cons come in uh
+// the conversions of one cell as values: from the hydro cons uh and the cell
+// field (FROMUTORVE's primitives, CUSTOM_CHECKRHO on the interior, P_to_U's
+// cons and UPDATE's pressure); FROM_CONS false starts from the primitives
+// rho, v and eps given in uh instead (initial_update)
+struct CellConv {
+    double u[5];      // cons after the floors
+    double w[4];      // rho, vx, vy, vz
+    double eps, p;    // p on the interior only
+    bool bad;         // non-finite density, velocity or pressure (interior)
+};
 template <int MODEL, bool FROM_CONS>
-__device__ __forceinline__ void utop_point(const UtopArgs& a, int i, bool interior, const double* uh, double bx,
-                                           double by, double bz, double* prim_out = nullptr) {
+__device__ __forceinline__ CellConv utop_of(const double* uh, bool interior, double bx, double by, double bz,
+                                            double ggas, double rho_floor, double eps_floor) {
+    CellConv o;
     const double bsquare = (bx * bx + by * by) + bz * bz;
     double rho, vx, vy, vz, e;
     if (FROM_CONS) {
@@ -410,41 +427,70 @@ __device__ __forceinline__ void utop_point(const UtopArgs& a, int i, bool interi
         const double vsquare = (vx * vx + vy * vy) + vz * vz;
         e = (uh[ITAU] - 0.5 * bsquare) / rho - 0.5 * vsquare;
     } else {
-        rho = a.w[0][i];
-        vx = a.w[1][i];
-        vy = a.w[2][i];
-        vz = a.w[3][i];
-        e = a.eps[i];
+        rho = uh[0];
+        vx = uh[1];
+        vy = uh[2];
+        vz = uh[3];
+        e = uh[4];
     }
     if (interior) {  // CUSTOM_CHECKRHO
         if (MODEL == 1) {
             e = fmax(e, 0.0);
         } else if (MODEL == 2 || MODEL == 3) {
-            if (rho < a.rho_floor) rho = a.rho_floor;
-            if (e < a.eps_floor) e = a.eps_floor;
+            if (rho < rho_floor) rho = rho_floor;
+            if (e < eps_floor) e = eps_floor;
         }
     }
     const double vsquare = (vx * vx + vy * vy) + vz * vz;
-    a.u[IRHO][i] = rho;
-    a.u[IVX][i] = vx * rho;
-    a.u[IVY][i] = vy * rho;
-    a.u[IVZ][i] = vz * rho;
-    a.u[ITAU][i] = rho * (e + 0.5 * vsquare) + 0.5 * bsquare;
-    a.w[0][i] = rho;
-    a.w[1][i] = vx;
-    a.w[2][i] = vy;
-    a.w[3][i] = vz;
-    a.eps[i] = e;
+    o.u[IRHO] = rho;
+    o.u[IVX] = vx * rho;
+    o.u[IVY] = vy * rho;
+    o.u[IVZ] = vz * rho;
+    o.u[ITAU] = rho * (e + 0.5 * vsquare) + 0.5 * bsquare;
+    o.w[0] = rho;
+    o.w[1] = vx;
+    o.w[2] = vy;
+    o.w[3] = vz;
+    o.eps = e;
+    o.p = 0.0;
+    o.bad = false;
     if (interior) {
-        const double p = (rho * e) * (a.ggas - 1.0);  // EOS_PRESSURE
-        a.w[4][i] = p;
-        if (!(isfinite(p) && isfinite(vsquare) && isfinite(rho))) atomicOr(a.flag, 1u);
+        o.p = (rho * e) * (ggas - 1.0);  // EOS_PRESSURE
+        o.bad = !(isfinite(o.p) && isfinite(vsquare) && isfinite(rho));
+    }
+    return o;
+}
+
+// the conversions of one cell; with FROM_CONS the hydro cons come in uh
+template <int MODEL, bool FROM_CONS>
+__device__ __forceinline__ void utop_point(const UtopArgs& a, int i, bool interior, const double* uh, double bx,
+                                           double by, double bz, double* prim_out = nullptr) {
+    double in[5];
+    if (FROM_CONS) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) in[q] = uh[q];
+    } else {
+        in[0] = a.w[0][i];
+        in[1] = a.w[1][i];
+        in[2] = a.w[2][i];
+        in[3] = a.w[3][i];
+        in[4] = a.eps[i];
+    }
+    const CellConv o = utop_of<MODEL, FROM_CONS>(in, interior, bx, by, bz, a.ggas, a.rho_floor, a.eps_floor);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) a.u[q][i] = o.u[q];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a.w[q][i] = o.w[q];
+    a.eps[i] = o.eps;
+    if (interior) {
+        a.w[4][i] = o.p;
+        if (o.bad) atomicOr(a.flag, 1u);
         if (prim_out) {
-            prim_out[0] = rho;
-            prim_out[1] = vx;
-            prim_out[2] = vy;
-            prim_out[3] = vz;
-            prim_out[4] = p;
+            prim_out[0] = o.w[0];
+            prim_out[1] = o.w[1];
+            prim_out[2] = o.w[2];
+            prim_out[3] = o.w[3];
+            prim_out[4] = o.p;
         }
     }
 }
@@ -497,6 +543,165 @@ __global__ void __launch_bounds__(256, 8) k_combine_utop(Box b, Tabs T, Prim pr,
         utop_point<MODEL, true>(o, i, interior, uh, bx, by, bz, fuse_dt ? pw : nullptr);
         if (fuse_dt && interior)
             dt_cell = cell_dt<COORD>(T, j, k, l, pw[0], pw[4], pw[1], pw[2], pw[3], bx, by, bz, o.ggas, o.cfl);
+    }
+    if (fuse_dt) block_min_dt(dt_cell, o.dtmin);
+}
+
+// k_combine_utop on two cells of a row per thread: cells j and j+1 with j
+// even, so that with an even row stride SX every pair index i = idx(j, k, l)
+// is even and each array is read and written as 16-byte pairs. The x
+// neighbour i-1 comes from the pair at i-2; the y and z neighbours i-SX and
+// i-SX*SY are pairs too. Every cell's value is the same expression, in the
+// same order, as in k_combine_utop (flux_diff, rk_point, utop_of), so the
+// results are bit for bit the scalar kernel's. A pair whose second cell lies
+// past nx (odd number of cells in the row) reads that in-box ghost index and
+// stores only the first cell; cells outside the interior keep their stored
+// bcell and pressure as in the scalar kernel. Needs SX even and every array
+// 16-byte aligned (checked by the launcher, which otherwise uses the scalar
+// kernel).
+__device__ __forceinline__ double2 ld2(const double* p, int i) {
+    return *reinterpret_cast<const double2*>(p + i);
+}
+__device__ __forceinline__ void st2(double* p, int i, double x, double y) {
+    *reinterpret_cast<double2*>(p + i) = make_double2(x, y);
+}
+
+template <int COORD, int MODEL, int STAGE>
+__global__ void __launch_bounds__(256, 4) k_combine_utop2(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy,
+                                                       FaceFlux fz, CombineArgs a, UtopArgs o) {
+    if (b.skip && *b.skip) return;
+    const int np = (b.nx + 2) >> 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = t < (long long)np * n1 * n2;
+    const bool fuse_dt = STAGE == 3 && o.dtmin;
+    if (!live && !fuse_dt) return;
+    double dt_cell = 1.0e10;
+    if (live) {
+        const int j = (int)(t % np) * 2, k = (int)((t / np) % n1), l = (int)(t / ((long long)np * n1));
+        const int i = b.idx(j, k, l);
+        const int sk = b.SX, sl = b.SX * b.SY;
+        const bool two = j + 1 <= b.nx;
+        const bool kl = k >= 1 && l >= 1;
+        const bool in0 = kl && j >= 1, in1 = kl && two;  // interior cells of the pair
+        double L0[5], L1[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) L0[q] = L1[q] = 0.0;
+        if (kl) {
+            double gp0, gc0, gm0, gp1, gc1, gm1;
+            geom_flux<COORD, 0>(T, j, k, l, gp0, gc0, gm0);
+            geom_flux<COORD, 0>(T, j + 1, k, l, gp1, gc1, gm1);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const double2 c = ld2(fx.f[q], i), m = ld2(fx.f[q], i - 2);
+                L0[q] = flux_diff(L0[q], c.x, m.y, gp0, gm0, gc0);
+                L1[q] = flux_diff(L1[q], c.y, c.x, gp1, gm1, gc1);
+            }
+            geom_flux<COORD, 1>(T, j, k, l, gp0, gc0, gm0);
+            geom_flux<COORD, 1>(T, j + 1, k, l, gp1, gc1, gm1);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const double2 c = ld2(fy.f[q], i), m = ld2(fy.f[q], i - sk);
+                L0[q] = flux_diff(L0[q], c.x, m.x, gp0, gm0, gc0);
+                L1[q] = flux_diff(L1[q], c.y, m.y, gp1, gm1, gc1);
+            }
+            geom_flux<COORD, 2>(T, j, k, l, gp0, gc0, gm0);
+            geom_flux<COORD, 2>(T, j + 1, k, l, gp1, gc1, gm1);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const double2 c = ld2(fz.f[q], i), m = ld2(fz.f[q], i - sl);
+                L0[q] = flux_diff(L0[q], c.x, m.x, gp0, gm0, gc0);
+                L1[q] = flux_diff(L1[q], c.y, m.y, gp1, gm1, gc1);
+            }
+            double sc[5];
+            if (in0) {
+                cell_sources<COORD, MODEL>(T, pr, a.geom_repeat, a.rho_floor, a.r_sh, j, k, l, i, sc);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) L0[q] = L0[q] + sc[q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) L0[q] = 0.0;
+            }
+            if (in1) {
+                cell_sources<COORD, MODEL>(T, pr, a.geom_repeat, a.rho_floor, a.r_sh, j + 1, k, l, i + 1, sc);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) L1[q] = L1[q] + sc[q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) L1[q] = 0.0;
+            }
+        }
+        const double dt = *a.dt;
+        double uh0[5], uh1[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double2 u0 = ld2(a.u0[q], i);
+            const double2 uc = STAGE == 1 ? make_double2(0.0, 0.0) : ld2(a.uc[q], i);
+            uh0[q] = rk_point<STAGE>(u0.x, uc.x, dt, L0[q]);
+            uh1[q] = rk_point<STAGE>(u0.y, uc.y, dt, L1[q]);
+            if (a.tape[q]) {
+                if (two) st2(a.tape[q], i, uh0[q], uh1[q]);
+                else a.tape[q][i] = uh0[q];
+            }
+        }
+        // cell fields: the face averages on the interior, the stored bcell elsewhere
+        double bx0, by0, bz0, bx1, by1, bz1;
+        {
+            const double2 fxc = ld2(o.u[IBX], i), fxm = ld2(o.u[IBX], i - 2);
+            const double2 fyc = ld2(o.u[IBY], i), fym = ld2(o.u[IBY], i - sk);
+            const double2 fzc = ld2(o.u[IBZ], i), fzm = ld2(o.u[IBZ], i - sl);
+            double2 s0 = make_double2(0.0, 0.0), s1 = s0, s2 = s0;
+            if (!(in0 && in1)) {
+                s0 = ld2(o.bc[0], i);
+                s1 = ld2(o.bc[1], i);
+                s2 = ld2(o.bc[2], i);
+            }
+            bx0 = in0 ? 0.5 * (fxc.x + fxm.y) : s0.x;
+            by0 = in0 ? 0.5 * (fyc.x + fym.x) : s1.x;
+            bz0 = in0 ? 0.5 * (fzc.x + fzm.x) : s2.x;
+            bx1 = in1 ? 0.5 * (fxc.y + fxc.x) : s0.y;
+            by1 = in1 ? 0.5 * (fyc.y + fym.y) : s1.y;
+            bz1 = in1 ? 0.5 * (fzc.y + fzm.y) : s2.y;
+            if (in0 && in1) {
+                st2(o.bc[0], i, bx0, bx1);
+                st2(o.bc[1], i, by0, by1);
+                st2(o.bc[2], i, bz0, bz1);
+            } else if (in0) {
+                o.bc[0][i] = bx0;
+                o.bc[1][i] = by0;
+                o.bc[2][i] = bz0;
+            } else if (in1) {
+                o.bc[0][i + 1] = bx1;
+                o.bc[1][i + 1] = by1;
+                o.bc[2][i + 1] = bz1;
+            }
+        }
+        const CellConv c0 = utop_of<MODEL, true>(uh0, in0, bx0, by0, bz0, o.ggas, o.rho_floor, o.eps_floor);
+        const CellConv c1 = utop_of<MODEL, true>(uh1, in1, bx1, by1, bz1, o.ggas, o.rho_floor, o.eps_floor);
+        if (two) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) st2(o.u[q], i, c0.u[q], c1.u[q]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) st2(o.w[q], i, c0.w[q], c1.w[q]);
+            st2(o.eps, i, c0.eps, c1.eps);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) o.u[q][i] = c0.u[q];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) o.w[q][i] = c0.w[q];
+            o.eps[i] = c0.eps;
+        }
+        if (in0 && in1) st2(o.w[4], i, c0.p, c1.p);
+        else if (in0) o.w[4][i] = c0.p;
+        else if (in1) o.w[4][i + 1] = c1.p;
+        if ((in0 && c0.bad) || (in1 && c1.bad)) atomicOr(o.flag, 1u);
+        if (fuse_dt) {
+            if (in0)
+                dt_cell = cell_dt<COORD>(T, j, k, l, c0.w[0], c0.p, c0.w[1], c0.w[2], c0.w[3], bx0, by0, bz0, o.ggas,
+                                         o.cfl);
+            if (in1)
+                dt_cell = fmin(dt_cell, cell_dt<COORD>(T, j + 1, k, l, c1.w[0], c1.p, c1.w[1], c1.w[2], c1.w[3], bx1,
+                                                       by1, bz1, o.ggas, o.cfl));
+        }
     }
     if (fuse_dt) block_min_dt(dt_cell, o.dtmin);
 }

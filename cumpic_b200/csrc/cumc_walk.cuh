@@ -30,6 +30,14 @@
 namespace cumc {
 
 constexpr int WK_THREADS = 64;
+// resident blocks per SM the walker and the x sweep are compiled for (the
+// register budget a thread gets); build-time tunables
+#ifndef CUMC_WALK_MINB
+#define CUMC_WALK_MINB 8
+#endif
+#ifndef CUMC_XWARP_MINB
+#define CUMC_XWARP_MINB 8
+#endif
 constexpr int WK_FIELDS = 7;  // rho, vx, vy, vz, p and the two tangential cell fields
 
 template <int DIR>
@@ -329,7 +337,7 @@ constexpr size_t walk_smem(int dir) {
 // c_lo, c_cnt: the columns walked (WalkCol; c_cnt < 0 for all)
 // RECIP: the HLL solve's quotients as products with reciprocals (hll_flux7)
 template <int DIR, int RECON, typename R, bool STATES = false, bool RECIP = false>
-__global__ void __launch_bounds__(WK_THREADS) k_sweep_walk_sm(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
+__global__ void __launch_bounds__(WK_THREADS, CUMC_WALK_MINB) k_sweep_walk_sm(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
                                                              int seg, FaceFluxT<R> out_r, int c_lo, int c_cnt) {
     static_assert(!STATES || DIR != 0, "face states along y and z");
     extern __shared__ __align__(16) unsigned char wk_raw[];
@@ -428,7 +436,7 @@ constexpr int XW_FACES = 27;
 // out_r, field order of the sweep) instead of solving HLL.
 // The rows are those of the z planes l_lo .. l_lo + l_cnt - 1 (l_cnt < 0: all).
 template <int RECON, typename R, bool STATES = false, bool RECIP = false>
-__global__ void __launch_bounds__(128, 8) k_sweep_xwarp(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
+__global__ void __launch_bounds__(128, CUMC_XWARP_MINB) k_sweep_xwarp(Box b, Tabs T, PrimT<R> pr, R ggas, FaceFluxT<R> out,
                                                         FaceFluxT<R> out_r, int l_lo, int l_cnt) {
     constexpr unsigned FULL = 0xffffffffu;
     const int nw = (b.nx + 1 + XW_FACES - 1) / XW_FACES;  // warps per row
