@@ -92,17 +92,74 @@ __device__ __forceinline__ void ec_edges(const Box& b, const FaceFlux& fx, const
     }
 }
 
+// the flux half of one edge's three EMFs (the first two sums of each, k_emf's
+// order); the cell-EMF half is added once the plane's cell EMFs are in
+// shared memory (ec_edge_finish)
+struct EdgePart {
+    double x, y, z;
+};
+__device__ __forceinline__ EdgePart ec_edge_part(const Box& b, const FaceFlux& fx, const FaceFlux& fy,
+                                                 const FaceFlux& fz, int j0, int k0, int l, int t) {
+    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
+    const double q = 0.25;
+    const int j = j0 - 1 + t % EC_EX, k = k0 - 1 + t / EC_EX;
+    EdgePart e{0.0, 0.0, 0.0};
+    if (j >= 0 && k >= 0 && j <= b.nx && k <= b.ny && l <= b.nz) {
+        const int i = b.idx(j, k, l);
+        e.x = 0.0 + q * (-fy.f[6][i] - fy.f[6][i + sl]);
+        e.x = e.x + q * (fz.f[6][i] + fz.f[6][i + sk]);
+        e.y = 0.0 + q * (fx.f[6][i] + fx.f[6][i + sl]);
+        e.y = e.y + q * (-fz.f[5][i] - fz.f[5][i + sj]);
+        e.z = 0.0 + q * (-fx.f[5][i] - fx.f[5][i + sk]);
+        e.z = e.z + q * (fy.f[5][i] + fy.f[5][i + sj]);
+    }
+    return e;
+}
+__device__ __forceinline__ void ec_edge_finish(const Box& b, EmfCtSmem& S, const EdgePart& e, int j0, int k0, int l,
+                                               int t) {
+    const double q = 0.25;
+    const int ej = t % EC_EX, ek = t / EC_EX;
+    const int j = j0 - 1 + ej, k = k0 - 1 + ek;
+    const bool live = j >= 0 && k >= 0 && j <= b.nx && k <= b.ny && l <= b.nz;
+    const int c0 = l & 1, c1 = (l + 1) & 1, cj = ej, ck = ek;
+    double ex = 0.0, ey = 0.0, ez = 0.0;
+    if (live) {
+        ex = e.x * 2.0 - q * (((S.ec[c0][0][ck][cj] + S.ec[c1][0][ck][cj]) + S.ec[c0][0][ck + 1][cj]) +
+                              S.ec[c1][0][ck + 1][cj]);
+        ey = e.y * 2.0 - q * (((S.ec[c0][1][ck][cj] + S.ec[c1][1][ck][cj]) + S.ec[c0][1][ck][cj + 1]) +
+                              S.ec[c1][1][ck][cj + 1]);
+        ez = e.z * 2.0 - q * (((S.ec[c0][2][ck][cj] + S.ec[c0][2][ck + 1][cj]) + S.ec[c0][2][ck][cj + 1]) +
+                              S.ec[c0][2][ck + 1][cj + 1]);
+    }
+    S.ex[l & 1][ek][ej] = ex;
+    S.ey[l & 1][ek][ej] = ey;
+    S.ez[ek][ej] = ez;
+}
+
+// Per plane a thread first issues its global loads (the flux half of its
+// edges, u_old and u of its face triple, the cell fields of its cells of the
+// next plane), so that one memory latency a plane is exposed instead of
+// three. Two barriers a plane: the next plane's cell EMFs overwrite the slot
+// of plane l-1's cells, read only before this plane's second barrier, and
+// its edges overwrite slots that CT reads, which every thread has finished
+// before it reaches the next plane's first barrier.
+#ifndef CUMC_EC_MINB
+#define CUMC_EC_MINB 4
+#endif
 template <int COORD, int STAGE>
-__global__ void __launch_bounds__(EC_TX * EC_TY, 6) k_emf_ct(Box b, Tabs T, Prim pr, FaceFlux fx, FaceFlux fy,
-                                                          FaceFlux fz, CombineArgs a) {
+__global__ void __launch_bounds__(EC_TX * EC_TY, CUMC_EC_MINB) k_emf_ct(Box b, Tabs T, Prim pr, FaceFlux fx,
+                                                                      FaceFlux fy, FaceFlux fz, CombineArgs a) {
     extern __shared__ __align__(16) unsigned char ec_raw[];
     EmfCtSmem& S = *reinterpret_cast<EmfCtSmem*>(ec_raw);
     if (b.skip && *b.skip) return;
+    constexpr int NE = EC_EX * EC_EY, NT = EC_TX * EC_TY;
+    static_assert(NE > NT && NE <= 2 * NT, "two edges a thread at most");
     const int j0 = blockIdx.x * EC_TX, k0 = blockIdx.y * EC_TY;
     const int l0 = blockIdx.z * EC_SEG, l1 = min(l0 + EC_SEG, b.nz + 1);
     const int tj = threadIdx.x % EC_TX, tk = threadIdx.x / EC_TX;
     const int j = j0 + tj, k = k0 + tk;
     const bool mine = j <= b.nx && k <= b.ny;
+    const int e0 = threadIdx.x, e1 = threadIdx.x + NT;  // the thread's edges (e1 < NE for some)
     const double dt = *a.dt;
 
     // prologue: the x and y edges of plane l0 - 1 (zero for l0 = 0)
@@ -112,9 +169,21 @@ __global__ void __launch_bounds__(EC_TX * EC_TY, 6) k_emf_ct(Box b, Tabs T, Prim
     ec_edges(b, fx, fy, fz, S, j0, k0, l0 - 1, false);
     __syncthreads();
     for (int l = l0; l < l1; ++l) {
+        const EdgePart p0 = ec_edge_part(b, fx, fy, fz, j0, k0, l, e0);
+        const EdgePart p1 = e1 < NE ? ec_edge_part(b, fx, fy, fz, j0, k0, l, e1) : EdgePart{0.0, 0.0, 0.0};
+        double u0v[3] = {0.0, 0.0, 0.0}, ucv[3] = {0.0, 0.0, 0.0};
+        const int i = b.idx(j, k, l);
+        if (mine) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                u0v[c] = a.u0[IBX + c][i];
+                if (STAGE != 1) ucv[c] = a.uc[IBX + c][i];
+            }
+        }
         ec_cells(b, pr, S, j0, k0, l + 1);  // replaces plane l - 1's cells
         __syncthreads();
-        ec_edges(b, fx, fy, fz, S, j0, k0, l, true);
+        ec_edge_finish(b, S, p0, j0, k0, l, e0);
+        if (e1 < NE) ec_edge_finish(b, S, p1, j0, k0, l, e1);
         __syncthreads();
         if (mine) {
             // ct_lrk (solver/mhd.f90:137-148) on the shared-memory edges; the tile's
@@ -129,15 +198,13 @@ __global__ void __launch_bounds__(EC_TX * EC_TY, 6) k_emf_ct(Box b, Tabs T, Prim
             L[0] = -((Ez * g.bx_ez_p - Ez_km * g.bx_ez_m) / g.bx_ez_c - (Ey * g.bx_ey_p - Ey_lm * g.bx_ey_m) / g.bx_ey_c);
             L[1] = -((Ex * g.by_ex_p - Ex_lm * g.by_ex_m) / g.by_ex_c - (Ez * g.by_ez_p - Ez_jm * g.by_ez_m) / g.by_ez_c);
             L[2] = -((Ey * g.bz_ey_p - Ey_jm * g.bz_ey_m) / g.bz_ey_c - (Ex * g.bz_ex_p - Ex_km * g.bz_ex_m) / g.bz_ex_c);
-            const int i = b.idx(j, k, l);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const double r = rk_point<STAGE>(a.u0[IBX + c][i], STAGE == 1 ? 0.0 : a.uc[IBX + c][i], dt, L[c]);
+                const double r = rk_point<STAGE>(u0v[c], ucv[c], dt, L[c]);
                 a.ud[IBX + c][i] = r;
                 if (a.tape[IBX + c]) a.tape[IBX + c][i] = r;
             }
         }
-        __syncthreads();  // the next plane overwrites the z edges and a cell-EMF slot
     }
 }
 

@@ -236,6 +236,104 @@ __device__ __forceinline__ void walk_step(const AxisTabs& A, int f, R v0, R v1, 
     }
 }
 
+// HLL of the mixed form from FP32 states in the reciprocal form of hll_flux7,
+// with the signal speeds evaluated in TS, the two sides' conserved values and
+// fluxes in TF and the HLL combination in TC (each float or double)
+template <int DIR, typename TS, typename TF, typename TC, bool ROUND = false>
+__device__ __forceinline__ void hll_flux7_mx(const float (&wl)[8], const float (&wr)[8], float ggas, float (&out)[7]) {
+    constexpr int ivn = IVX + DIR;
+    constexpr int ibn = IBX + DIR, ibt1 = IBX + (DIR + 1) % 3, ibt2 = IBX + (DIR + 2) % 3;
+    TS sL, sR;
+    {
+        const TS g = (TS)ggas;
+        const TS rL = wl[IRHO], rR = wr[IRHO];
+        const TS irL = TS(1) / rL, irR = TS(1) / rR;
+        const TS csL = sqrt((g * (TS)wl[ITAU]) * irL);
+        const TS csR = sqrt((g * (TS)wr[ITAU]) * irR);
+        const TS cfsL = signalspeed_recip<TS>(csL, wl[ibn], wl[ibt1], wl[ibt2], irL);
+        const TS cfsR = signalspeed_recip<TS>(csR, wr[ibn], wr[ibt1], wr[ibt2], irR);
+        const TS sqL = sqrt(rL), sqR = sqrt(rR);
+        const TS isq = TS(1) / (sqL + sqR);
+        const TS ubar = (sqL * (TS)wl[ivn] + sqR * (TS)wr[ivn]) * isq;
+        const TS cbar = (sqL * cfsL + sqR * cfsR) * isq;
+        sL = fmin((TS)wl[ivn] - cfsL, ubar - cbar);
+        sR = fmax((TS)wr[ivn] + cfsR, ubar + cbar);
+    }
+    TF a[8], c[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        a[q] = wl[q];
+        c[q] = wr[q];
+    }
+    using Side = FaceSide<DIR, TF>;
+    const TF ig = TF(1) / ((TF)ggas - TF(1));
+    Side L(a, a[ITAU] * (TF(1) / a[IRHO]) * ig, typename Side::GivenEps{});
+    Side Rs(c, c[ITAU] * (TF(1) / c[IRHO]) * ig, typename Side::GivenEps{});
+    if (ROUND) {  // the derived side scalars rounded to FP32
+        L.E = (float)L.E;
+        L.hb2 = (float)L.hb2;
+        L.vdotb = (float)L.vdotb;
+        Rs.E = (float)Rs.E;
+        Rs.hb2 = (float)Rs.hb2;
+        Rs.vdotb = (float)Rs.vdotb;
+    }
+    constexpr int bt_a = DIR == 0 ? IBY : IBX;
+    constexpr int bt_b = DIR == 2 ? IBY : IBZ;
+    const int comp[7] = {IRHO, IVX, IVY, IVZ, ITAU, bt_a, bt_b};
+    if (sL >= TS(0)) {
+#pragma unroll
+        for (int q = 0; q < 7; ++q) out[q] = (float)L.f(comp[q]);
+    } else if (sR >= TS(0)) {
+        const TC cl = (TC)sL, cr = (TC)sR;
+        const TC ids = TC(1) / (cr - cl), lr = cl * cr;
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            const TC yl = (TC)L.f(comp[q]), yr = (TC)Rs.f(comp[q]), xl = (TC)L.u(comp[q]), xr = (TC)Rs.u(comp[q]);
+            out[q] = (float)(((cr * yl - cl * yr) + lr * (xr - xl)) * ids);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 7; ++q) out[q] = (float)Rs.f(comp[q]);
+    }
+}
+
+// the sweeps' HLL solve. A mixed-unit build with CUMC_MX_HLL64 defined widens
+// the FP32 states and solves in FP64, rounding the fluxes to FP32 (a build
+// that measures how much of the mixed form's error the FP32 solve makes).
+template <int DIR, typename R, bool RECIP>
+__device__ __forceinline__ void sweep_hll(const R (&wl)[8], const R (&wr)[8], R ggas, R (&fx)[7]) {
+#ifdef CUMC_MX_HLL64
+    if constexpr (sizeof(R) == 4) {
+        double a[8], c[8], o[7];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            a[q] = (double)wl[q];
+            c[q] = (double)wr[q];
+        }
+        hll_flux7<DIR, double, RECIP>(a, c, (double)ggas, o);
+#pragma unroll
+        for (int q = 0; q < 7; ++q) fx[q] = (R)o[q];
+        return;
+    }
+#endif
+#ifdef CUMC_MX_PREC  // four digits: speeds, sides, combination (4 float, 8 double), side scalars rounded (1)
+    if constexpr (sizeof(R) == 4) {
+        using TS = std::conditional_t<(CUMC_MX_PREC / 1000) == 8, double, float>;
+        using TF = std::conditional_t<(CUMC_MX_PREC / 100 % 10) == 8, double, float>;
+        using TC = std::conditional_t<(CUMC_MX_PREC / 10 % 10) == 8, double, float>;
+        hll_flux7_mx<DIR, TS, TF, TC, (CUMC_MX_PREC % 10) == 1>(wl, wr, ggas, fx);
+        return;
+    }
+#endif
+#ifdef CUMC_MX_RECIP
+    if constexpr (sizeof(R) == 4) {
+        hll_flux7<DIR, R, true>(wl, wr, ggas, fx);
+        return;
+    }
+#endif
+    hll_flux7<DIR, R, RECIP>(wl, wr, ggas, fx);
+}
+
 // HLL at face f; the x sweep parks the fluxes in the staging slots (j)
 template <int DIR, typename R, bool RECIP = false>
 __device__ __forceinline__ void walk_flux(const WalkCol<DIR, R>& C, int f, R (&wl)[8], R (&wr)[8], R ggas,
@@ -243,7 +341,7 @@ __device__ __forceinline__ void walk_flux(const WalkCol<DIR, R>& C, int f, R (&w
     wl[IBX + DIR] = bn;
     wr[IBX + DIR] = bn;
     R fx[7];
-    hll_flux7<DIR, R, RECIP>(wl, wr, ggas, fx);
+    sweep_hll<DIR, R, RECIP>(wl, wr, ggas, fx);
     if (DIR == 0) {
 #pragma unroll
         for (int i = 0; i < 7; ++i) X.put(i, j, fx[i]);
@@ -488,7 +586,7 @@ __global__ void __launch_bounds__(128, CUMC_XWARP_MINB) k_sweep_xwarp(Box b, Tab
     wl[IBX] = bn;
     wr[IBX] = bn;
     R fx[7];
-    hll_flux7<0, R, RECIP>(wl, wr, ggas, fx);
+    sweep_hll<0, R, RECIP>(wl, wr, ggas, fx);
 #pragma unroll
     for (int i = 0; i < 7; ++i) out.f[i][base + c] = fx[i];
 }
