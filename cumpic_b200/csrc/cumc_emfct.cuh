@@ -25,20 +25,25 @@ constexpr int EC_CX = EC_TX + 2, EC_CY = EC_TY + 2;  // cells j0-1..j0+32, k0-1.
 constexpr int EC_EX = EC_TX + 1, EC_EY = EC_TY + 1;  // edges j0-1..j0+31, k0-1..k0+7
 constexpr int EC_SEG = 32;                     // planes a block marches over
 
-struct EmfCtSmem {
-    double ec[2][3][EC_CY][EC_CX];   // cell EMFs of two planes (ring by plane parity)
-    double ex[2][EC_EY][EC_EX];      // x edge EMFs of two planes (ring by plane parity)
-    double ey[2][EC_EY][EC_EX];      // y edge EMFs of two planes
-    double ez[EC_EY][EC_EX];         // z edge EMFs of the current plane
+// shared memory of a tile; R is the EMFs' type (double, or float in the
+// mixed form)
+template <typename R>
+struct EmfCtSmemT {
+    R ec[2][3][EC_CY][EC_CX];   // cell EMFs of two planes (ring by plane parity)
+    R ex[2][EC_EY][EC_EX];      // x edge EMFs of two planes (ring by plane parity)
+    R ey[2][EC_EY][EC_EX];      // y edge EMFs of two planes
+    R ez[EC_EY][EC_EX];         // z edge EMFs of the current plane
 };
+using EmfCtSmem = EmfCtSmemT<double>;
 
 // cell EMFs of plane l for the tile's cells (zero outside -1..n+1)
-__device__ __forceinline__ void ec_cells(const Box& b, const Prim& pr, EmfCtSmem& S, int j0, int k0, int l) {
+template <typename R>
+__device__ __forceinline__ void ec_cells(const Box& b, const PrimT<R>& pr, EmfCtSmemT<R>& S, int j0, int k0, int l) {
     const int slot = l & 1;
     for (int t = threadIdx.x; t < EC_CX * EC_CY; t += EC_TX * EC_TY) {
         const int cj = t % EC_CX, ck = t / EC_CX;
         const int j = j0 - 1 + cj, k = k0 - 1 + ck;
-        double x = 0.0, y = 0.0, z = 0.0;
+        R x = R(0), y = R(0), z = R(0);
         if (j <= b.nx + 1 && k <= b.ny + 1 && l >= -1 && l <= b.nz + 1) {
             const int i = b.idx(j, k, l);
             x = ecell_x(pr, i);
@@ -52,10 +57,11 @@ __device__ __forceinline__ void ec_cells(const Box& b, const Prim& pr, EmfCtSmem
 }
 
 // edge EMFs of plane l (x and y edges into their ring slot; z edges with `z`)
-__device__ __forceinline__ void ec_edges(const Box& b, const FaceFlux& fx, const FaceFlux& fy, const FaceFlux& fz,
-                                         EmfCtSmem& S, int j0, int k0, int l, bool z) {
+template <typename R>
+__device__ __forceinline__ void ec_edges(const Box& b, const FaceFluxT<R>& fx, const FaceFluxT<R>& fy,
+                                         const FaceFluxT<R>& fz, EmfCtSmemT<R>& S, int j0, int k0, int l, bool z) {
     const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
-    const double q = 0.25;
+    const R q = R(0.25);
     const int c0 = l & 1, c1 = (l + 1) & 1;  // cell-EMF slots of planes l and l+1
     const int e = l & 1;
     for (int t = threadIdx.x; t < EC_EX * EC_EY; t += EC_TX * EC_TY) {
@@ -66,23 +72,23 @@ __device__ __forceinline__ void ec_edges(const Box& b, const FaceFlux& fx, const
         // cell (j, k) of the edge is cell slot (ck, cj) = (ek, ej): the edge sits
         // at the upper faces of cells j and k
         const int cj = ej, ck = ek;
-        double ex = 0.0, ey = 0.0, ez = 0.0;
+        R ex = R(0), ey = R(0), ez = R(0);
         if (live) {
-            ex = 0.0 + q * (-fy.f[6][i] - fy.f[6][i + sl]);
+            ex = R(0) + q * (-fy.f[6][i] - fy.f[6][i + sl]);
             ex = ex + q * (fz.f[6][i] + fz.f[6][i + sk]);
-            ey = 0.0 + q * (fx.f[6][i] + fx.f[6][i + sl]);
+            ey = R(0) + q * (fx.f[6][i] + fx.f[6][i + sl]);
             ey = ey + q * (-fz.f[5][i] - fz.f[5][i + sj]);
             // k_emf's sums: cells (j,k,l), (j,k,l+1), (j,k+1,l), (j,k+1,l+1) for Ex;
             // (j,k,l), (j,k,l+1), (j+1,k,l), (j+1,k,l+1) for Ey; (j,k), (j,k+1),
             // (j+1,k), (j+1,k+1) of plane l for Ez
-            ex = ex * 2.0 - q * (((S.ec[c0][0][ck][cj] + S.ec[c1][0][ck][cj]) + S.ec[c0][0][ck + 1][cj]) +
+            ex = ex * R(2) - q * (((S.ec[c0][0][ck][cj] + S.ec[c1][0][ck][cj]) + S.ec[c0][0][ck + 1][cj]) +
                                  S.ec[c1][0][ck + 1][cj]);
-            ey = ey * 2.0 - q * (((S.ec[c0][1][ck][cj] + S.ec[c1][1][ck][cj]) + S.ec[c0][1][ck][cj + 1]) +
+            ey = ey * R(2) - q * (((S.ec[c0][1][ck][cj] + S.ec[c1][1][ck][cj]) + S.ec[c0][1][ck][cj + 1]) +
                                  S.ec[c1][1][ck][cj + 1]);
             if (z) {
-                ez = 0.0 + q * (-fx.f[5][i] - fx.f[5][i + sk]);
+                ez = R(0) + q * (-fx.f[5][i] - fx.f[5][i + sk]);
                 ez = ez + q * (fy.f[5][i] + fy.f[5][i + sj]);
-                ez = ez * 2.0 - q * (((S.ec[c0][2][ck][cj] + S.ec[c0][2][ck + 1][cj]) + S.ec[c0][2][ck][cj + 1]) +
+                ez = ez * R(2) - q * (((S.ec[c0][2][ck][cj] + S.ec[c0][2][ck + 1][cj]) + S.ec[c0][2][ck][cj + 1]) +
                                      S.ec[c0][2][ck + 1][cj + 1]);
             }
         }
@@ -95,41 +101,44 @@ __device__ __forceinline__ void ec_edges(const Box& b, const FaceFlux& fx, const
 // the flux half of one edge's three EMFs (the first two sums of each, k_emf's
 // order); the cell-EMF half is added once the plane's cell EMFs are in
 // shared memory (ec_edge_finish)
+template <typename R>
 struct EdgePart {
-    double x, y, z;
+    R x, y, z;
 };
-__device__ __forceinline__ EdgePart ec_edge_part(const Box& b, const FaceFlux& fx, const FaceFlux& fy,
-                                                 const FaceFlux& fz, int j0, int k0, int l, int t) {
+template <typename R>
+__device__ __forceinline__ EdgePart<R> ec_edge_part(const Box& b, const FaceFluxT<R>& fx, const FaceFluxT<R>& fy,
+                                                    const FaceFluxT<R>& fz, int j0, int k0, int l, int t) {
     const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
-    const double q = 0.25;
+    const R q = R(0.25);
     const int j = j0 - 1 + t % EC_EX, k = k0 - 1 + t / EC_EX;
-    EdgePart e{0.0, 0.0, 0.0};
+    EdgePart<R> e{R(0), R(0), R(0)};
     if (j >= 0 && k >= 0 && j <= b.nx && k <= b.ny && l <= b.nz) {
         const int i = b.idx(j, k, l);
-        e.x = 0.0 + q * (-fy.f[6][i] - fy.f[6][i + sl]);
+        e.x = R(0) + q * (-fy.f[6][i] - fy.f[6][i + sl]);
         e.x = e.x + q * (fz.f[6][i] + fz.f[6][i + sk]);
-        e.y = 0.0 + q * (fx.f[6][i] + fx.f[6][i + sl]);
+        e.y = R(0) + q * (fx.f[6][i] + fx.f[6][i + sl]);
         e.y = e.y + q * (-fz.f[5][i] - fz.f[5][i + sj]);
-        e.z = 0.0 + q * (-fx.f[5][i] - fx.f[5][i + sk]);
+        e.z = R(0) + q * (-fx.f[5][i] - fx.f[5][i + sk]);
         e.z = e.z + q * (fy.f[5][i] + fy.f[5][i + sj]);
     }
     return e;
 }
-__device__ __forceinline__ void ec_edge_finish(const Box& b, EmfCtSmem& S, const EdgePart& e, int j0, int k0, int l,
-                                               int t) {
-    const double q = 0.25;
+template <typename R>
+__device__ __forceinline__ void ec_edge_finish(const Box& b, EmfCtSmemT<R>& S, const EdgePart<R>& e, int j0, int k0,
+                                               int l, int t) {
+    const R q = R(0.25);
     const int ej = t % EC_EX, ek = t / EC_EX;
     const int j = j0 - 1 + ej, k = k0 - 1 + ek;
     const bool live = j >= 0 && k >= 0 && j <= b.nx && k <= b.ny && l <= b.nz;
     const int c0 = l & 1, c1 = (l + 1) & 1, cj = ej, ck = ek;
-    double ex = 0.0, ey = 0.0, ez = 0.0;
+    R ex = R(0), ey = R(0), ez = R(0);
     if (live) {
-        ex = e.x * 2.0 - q * (((S.ec[c0][0][ck][cj] + S.ec[c1][0][ck][cj]) + S.ec[c0][0][ck + 1][cj]) +
-                              S.ec[c1][0][ck + 1][cj]);
-        ey = e.y * 2.0 - q * (((S.ec[c0][1][ck][cj] + S.ec[c1][1][ck][cj]) + S.ec[c0][1][ck][cj + 1]) +
-                              S.ec[c1][1][ck][cj + 1]);
-        ez = e.z * 2.0 - q * (((S.ec[c0][2][ck][cj] + S.ec[c0][2][ck + 1][cj]) + S.ec[c0][2][ck][cj + 1]) +
-                              S.ec[c0][2][ck + 1][cj + 1]);
+        ex = e.x * R(2) - q * (((S.ec[c0][0][ck][cj] + S.ec[c1][0][ck][cj]) + S.ec[c0][0][ck + 1][cj]) +
+                               S.ec[c1][0][ck + 1][cj]);
+        ey = e.y * R(2) - q * (((S.ec[c0][1][ck][cj] + S.ec[c1][1][ck][cj]) + S.ec[c0][1][ck][cj + 1]) +
+                               S.ec[c1][1][ck][cj + 1]);
+        ez = e.z * R(2) - q * (((S.ec[c0][2][ck][cj] + S.ec[c0][2][ck + 1][cj]) + S.ec[c0][2][ck][cj + 1]) +
+                               S.ec[c0][2][ck + 1][cj + 1]);
     }
     S.ex[l & 1][ek][ej] = ex;
     S.ey[l & 1][ek][ej] = ey;
@@ -169,8 +178,8 @@ __global__ void __launch_bounds__(EC_TX * EC_TY, CUMC_EC_MINB) k_emf_ct(Box b, T
     ec_edges(b, fx, fy, fz, S, j0, k0, l0 - 1, false);
     __syncthreads();
     for (int l = l0; l < l1; ++l) {
-        const EdgePart p0 = ec_edge_part(b, fx, fy, fz, j0, k0, l, e0);
-        const EdgePart p1 = e1 < NE ? ec_edge_part(b, fx, fy, fz, j0, k0, l, e1) : EdgePart{0.0, 0.0, 0.0};
+        const EdgePart<double> p0 = ec_edge_part(b, fx, fy, fz, j0, k0, l, e0);
+        const EdgePart<double> p1 = e1 < NE ? ec_edge_part(b, fx, fy, fz, j0, k0, l, e1) : EdgePart<double>{0.0, 0.0, 0.0};
         double u0v[3] = {0.0, 0.0, 0.0}, ucv[3] = {0.0, 0.0, 0.0};
         const int i = b.idx(j, k, l);
         if (mine) {

@@ -1,12 +1,18 @@
 // cumc_mixed.cu — mixed-precision form of the CUMC3D step (CUMC_MIXED).
 //
-// Compiled separately from the FP64 path, with FMA contraction and fast FP32
-// division: nothing here is meant to be bit-compatible with the reference.
+// Compiled separately from the FP64 path, with FMA contraction (IEEE-rounded
+// FP32 division and square root): nothing here is meant to be bit-compatible
+// with the reference.
 //
 // What runs in which precision:
-//   * reconstruction, HLL fluxes, EMFs, flux differences, sources, CT curl: FP32
-//     (the tiled sweep and k_emf templates shared with the FP64 path);
-//   * the RK3 accumulation of rho, rho v and B: U^n is kept as a hi/lo pair of
+//   * reconstruction, the HLL wave speeds, the HLL flux of the tangential
+//     fields, EMFs, flux differences, sources: FP32 (the sweep and EMF
+//     templates shared with the FP64 path); the HLL flux of the five hydro
+//     components is combined in FP64 from the FP32 states (hll_flux7_mixed,
+//     cumc_walk.cuh), which halves the largest FP32 error left;
+//   * the CT curl of the FP32 edge EMFs and the face-field increments: FP64,
+//     so that div B stays at round-off;
+//   * the RK3 accumulation of rho and rho v: U^n is kept as a hi/lo pair of
 //     FP32 values and updated with Knuth's TwoSum and Dekker's FastTwoSum;
 //     stage states are stored as the FP32 increment d_s = U_s - U^n, so their
 //     rounding error scales with the increment, not with U;
@@ -17,7 +23,11 @@
 //   d1 = dt L1,  d2 = (d1 + dt L2)/4,  U^{n+1} = U^n + 2/3 (d2 + dt L3)
 // which equals u1 = u0 + dt L1, u2 = 3/4 u0 + 1/4 u1 + 1/4 dt L2,
 // u3 = 1/3 u0 + 2/3 u2 + 2/3 dt L3 in exact arithmetic.
+// A stage is the three sweeps, k_emf_ct_mx, k_combine_utop_mx and the
+// boundary fill (CUMC_MX_STAGE=split runs k_emf, k_combine_mx and k_utop_mx
+// instead, for A/B timing).
 #include "cumc_mixed.h"
+#include "cumc_emfct.cuh"
 #include "cumc_sweep.cuh"
 #include "cumc_walk.cuh"
 
@@ -78,21 +88,15 @@ struct CombineMx {
 // k_combine_mx and k_utop_mx wait on memory: 8 blocks of 256 per SM (a full
 // SM of warps, a few registers spilled) beat 5 unspilled ones (1.05 -> 0.77 ms
 // and 0.63 -> 0.54 ms at 256^3)
-template <int COORD, int MODEL, int STAGE>
-__global__ void __launch_bounds__(256, 8) k_combine_mx(Box b, Tabs T, FaceFluxT<float> fx, FaceFluxT<float> fy,
-                                                    FaceFluxT<float> fz, CombineMx a) {
-    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
-    const long long total = (long long)n0 * n1 * n2;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total || (b.skip && *b.skip)) return;
-    const int j = (int)(t % n0);
-    const int k = (int)((t / n0) % n1);
-    const int l = (int)(t / ((long long)n0 * n1));
-    const int i = b.idx(j, k, l);
+// hydro l_rk of cell (j, k, l) in FP32: flux differences and sources (zero
+// outside the interior)
+template <int COORD, int MODEL>
+__device__ __forceinline__ void hydro_l_mx(const Box& b, const Tabs& T, const FaceFluxT<float>& fx,
+                                           const FaceFluxT<float>& fy, const FaceFluxT<float>& fz, const CombineMx& a,
+                                           int j, int k, int l, int i, float* L) {
     const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
-    float L[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) L[q] = 0.f;
+    for (int q = 0; q < 5; ++q) L[q] = 0.f;
     if (j >= 1 && k >= 1 && l >= 1) {
         double gp, gc, gm;
         geom_flux<COORD, 0>(T, j, k, l, gp, gc, gm);
@@ -137,6 +141,30 @@ __global__ void __launch_bounds__(256, 8) k_combine_mx(Box b, Tabs T, FaceFluxT<
             L[ITAU] -= factor * rho * (vx * x + vz * z) * inv;
         }
     }
+}
+
+#ifndef CUMC_MXC_MINB
+#define CUMC_MXC_MINB 8
+#endif
+#ifndef CUMC_MXU_MINB
+#define CUMC_MXU_MINB 8
+#endif
+template <int COORD, int MODEL, int STAGE>
+__global__ void __launch_bounds__(256, CUMC_MXC_MINB) k_combine_mx(Box b, Tabs T, FaceFluxT<float> fx, FaceFluxT<float> fy,
+                                                    FaceFluxT<float> fz, CombineMx a) {
+    const int n0 = b.nx + 1, n1 = b.ny + 1, n2 = b.nz + 1;
+    const long long total = (long long)n0 * n1 * n2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total || (b.skip && *b.skip)) return;
+    const int j = (int)(t % n0);
+    const int k = (int)((t / n0) % n1);
+    const int l = (int)(t / ((long long)n0 * n1));
+    const int i = b.idx(j, k, l);
+    const int sj = 1, sk = b.SX, sl = b.SX * b.SY;
+    float L[8];
+#pragma unroll
+    for (int q = 5; q < 8; ++q) L[q] = 0.f;
+    hydro_l_mx<COORD, MODEL>(b, T, fx, fy, fz, a, j, k, l, i, L);
     // CT curl of the FP32 edge EMFs, formed in FP64 (solver/mhd.f90:137-148)
     double LB[3];
     {
@@ -191,6 +219,96 @@ __global__ void __launch_bounds__(256, 8) k_combine_mx(Box b, Tabs T, FaceFluxT<
     if (STAGE == 1) a.es[i] = a.e0[i] + dt * LE;
     else if (STAGE == 2) a.es[i] = (rk20 * a.e0[i] + rk21 * a.es[i]) + (rk22 * dt) * LE;
     else a.e0[i] = (rk30 * a.e0[i] + rk31 * a.es[i]) + (rk32 * dt) * LE;
+}
+
+// ---------------------------------------------------------------------------
+// The fused stage (default): k_emf_ct_mx forms the FP32 edge EMFs of a tile
+// in shared memory (the tiles and z march of k_emf_ct) and applies the CT
+// curl in FP64 to the face-field increments; k_combine_utop_mx then forms
+// the hydro combine of a cell in registers and converts it at once, as
+// k_combine_mx followed by k_utop_mx would (the same expressions in the same
+// order), so the hydro increments and the stage energy do not make a round
+// trip through HBM between the two and the edge EMFs never reach it.
+// ---------------------------------------------------------------------------
+struct CtMx {
+    float* uh[3];   // U^n face fields, high parts
+    float* ul[3];   // low parts
+    double* db[3];  // stage increments of the face fields
+    const double* dt;
+};
+
+#ifndef CUMC_ECMX_MINB
+#define CUMC_ECMX_MINB 6
+#endif
+template <int COORD, int STAGE>
+__global__ void __launch_bounds__(EC_TX * EC_TY, CUMC_ECMX_MINB) k_emf_ct_mx(Box b, Tabs T, PrimT<float> pr, FaceFluxT<float> fx,
+                                                               FaceFluxT<float> fy, FaceFluxT<float> fz, CtMx a) {
+    extern __shared__ __align__(16) unsigned char ecm_raw[];
+    EmfCtSmemT<float>& S = *reinterpret_cast<EmfCtSmemT<float>*>(ecm_raw);
+    if (b.skip && *b.skip) return;
+    constexpr int NE = EC_EX * EC_EY, NT = EC_TX * EC_TY;
+    const int j0 = blockIdx.x * EC_TX, k0 = blockIdx.y * EC_TY;
+    const int l0 = blockIdx.z * EC_SEG, l1 = min(l0 + EC_SEG, b.nz + 1);
+    const int tj = threadIdx.x % EC_TX, tk = threadIdx.x / EC_TX;
+    const int j = j0 + tj, k = k0 + tk;
+    const bool mine = j <= b.nx && k <= b.ny;
+    const int e0 = threadIdx.x, e1 = threadIdx.x + NT;
+    const double dt = *a.dt;
+
+    ec_cells(b, pr, S, j0, k0, l0 - 1);
+    ec_cells(b, pr, S, j0, k0, l0);
+    __syncthreads();
+    ec_edges(b, fx, fy, fz, S, j0, k0, l0 - 1, false);
+    __syncthreads();
+    for (int l = l0; l < l1; ++l) {
+        const EdgePart<float> p0 = ec_edge_part(b, fx, fy, fz, j0, k0, l, e0);
+        const EdgePart<float> p1 = e1 < NE ? ec_edge_part(b, fx, fy, fz, j0, k0, l, e1) : EdgePart<float>{0.f, 0.f, 0.f};
+        const int i = b.idx(j, k, l);
+        double dbv[3] = {0.0, 0.0, 0.0};
+        float hv[3] = {0.f, 0.f, 0.f}, lv[3] = {0.f, 0.f, 0.f};
+        if (mine) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                if (STAGE != 1) dbv[c] = a.db[c][i];
+                if (STAGE == 3) {
+                    hv[c] = a.uh[c][i];
+                    lv[c] = a.ul[c][i];
+                }
+            }
+        }
+        ec_cells(b, pr, S, j0, k0, l + 1);
+        __syncthreads();
+        ec_edge_finish(b, S, p0, j0, k0, l, e0);
+        if (e1 < NE) ec_edge_finish(b, S, p1, j0, k0, l, e1);
+        __syncthreads();
+        if (mine) {
+            // CT curl of the FP32 edge EMFs, formed in FP64 (solver/mhd.f90:137-148)
+            const int ej = tj + 1, ek = tk + 1, e = l & 1, em = (l - 1) & 1;
+            const double Ez = S.ez[ek][ej], Ez_km = S.ez[ek - 1][ej], Ez_jm = S.ez[ek][ej - 1];
+            const double Ey = S.ey[e][ek][ej], Ey_lm = S.ey[em][ek][ej], Ey_jm = S.ey[e][ek][ej - 1];
+            const double Ex = S.ex[e][ek][ej], Ex_lm = S.ex[em][ek][ej], Ex_km = S.ex[e][ek - 1][ej];
+            CTf g;
+            geom_ct<COORD>(T, j, k, l, g);
+            double LB[3];
+            LB[0] = -((Ez * g.bx_ez_p - Ez_km * g.bx_ez_m) / g.bx_ez_c - (Ey * g.bx_ey_p - Ey_lm * g.bx_ey_m) / g.bx_ey_c);
+            LB[1] = -((Ex * g.by_ex_p - Ex_lm * g.by_ex_m) / g.by_ex_c - (Ez * g.by_ez_p - Ez_jm * g.by_ez_m) / g.by_ez_c);
+            LB[2] = -((Ey * g.bz_ey_p - Ey_jm * g.bz_ey_m) / g.bz_ey_c - (Ex * g.bz_ex_p - Ex_km * g.bz_ex_m) / g.bz_ex_c);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                if (STAGE == 1) {
+                    a.db[c][i] = dt * LB[c];
+                } else if (STAGE == 2) {
+                    a.db[c][i] = 0.25 * (dbv[c] + dt * LB[c]);
+                } else {
+                    const double v = df_val(hv[c], lv[c]) + (2.0 / 3.0) * (dbv[c] + dt * LB[c]);
+                    float hi, lo;
+                    df_split(v, hi, lo);
+                    a.uh[c][i] = hi;
+                    a.ul[c][i] = lo;
+                }
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -296,7 +414,7 @@ __device__ __forceinline__ double utop_mx_cell(const Box& b, const Tabs& T, cons
 // the block reduction has one call site, which every thread of the block
 // reaches (its warp shuffles and barrier need all of them)
 template <int COORD, int MODEL, bool FINAL>
-__global__ void __launch_bounds__(256, 8) k_utop_mx(Box b, Tabs T, UtopMx a) {
+__global__ void __launch_bounds__(256, CUMC_MXU_MINB) k_utop_mx(Box b, Tabs T, UtopMx a) {
     const long long total = (long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1);
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b.skip && *b.skip) return;  // the same for every thread
@@ -304,6 +422,137 @@ __global__ void __launch_bounds__(256, 8) k_utop_mx(Box b, Tabs T, UtopMx a) {
     if (t >= total && !fuse_dt) return;
     double dt_cell = 1.0e10;
     if (t < total) dt_cell = utop_mx_cell<COORD, MODEL, FINAL>(b, T, a, t, fuse_dt);
+    if (fuse_dt) block_min_dt(dt_cell, a.dtmin);
+}
+
+// k_combine_mx's hydro part and k_utop_mx's conversion of one cell in one
+// pass: the new increments (or, at stage 3, the new hi/lo state) and stage
+// energy stay in registers between the two. The face fields come from
+// k_emf_ct_mx, which has written all of them (the cell field averages the
+// neighbours at i-1, i-SX and i-SX*SY). Every thread stays to the block's min
+// reduction when the stage-3 launch forms the next step's dt.
+#ifndef CUMC_CUMX_MINB
+#define CUMC_CUMX_MINB 6
+#endif
+template <int COORD, int MODEL, int STAGE>
+__global__ void __launch_bounds__(256, CUMC_CUMX_MINB) k_combine_utop_mx(Box b, Tabs T, FaceFluxT<float> fx, FaceFluxT<float> fy,
+                                                         FaceFluxT<float> fz, CombineMx c, UtopMx a) {
+    constexpr bool FINAL = STAGE == 3;
+    const int n0 = b.nx + 1, n1 = b.ny + 1;
+    const long long total = (long long)n0 * n1 * (b.nz + 1);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b.skip && *b.skip) return;
+    const bool fuse_dt = FINAL && a.dtmin;
+    if (t >= total && !fuse_dt) return;
+    double dt_cell = 1.0e10;
+    if (t < total) {
+        const int j = (int)(t % n0);
+        const int k = (int)((t / n0) % n1);
+        const int l = (int)(t / ((long long)n0 * n1));
+        const int i = b.idx(j, k, l);
+        const bool interior = j >= 1 && k >= 1 && l >= 1;
+        float L[5];
+        hydro_l_mx<COORD, MODEL>(b, T, fx, fy, fz, c, j, k, l, i, L);
+        const double dt = *c.dt;
+        const float dtf = (float)dt;
+        // the combine (k_combine_mx): new increments dn (stages 1, 2) or the new
+        // hi/lo state (stage 3) of rho and rho v; the stage energy
+        float uh4[4], ul4[4], dn[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uh4[q] = a.uh[q][i];
+            ul4[q] = a.ul[q][i];
+            if (STAGE == 1) {
+                dn[q] = dtf * L[q];
+            } else if (STAGE == 2) {
+                dn[q] = 0.25f * (a.d[q][i] + dtf * L[q]);
+            } else {
+                const float inc = (2.f / 3.f) * (a.d[q][i] + dtf * L[q]);
+                df_add(uh4[q], ul4[q], inc);
+                dn[q] = 0.f;
+            }
+        }
+        const double LE = (double)L[ITAU];
+        constexpr double rk20 = 3.0 / 4.0, rk21 = 1.0 / 4.0, rk22 = 1.0 / 4.0;
+        constexpr double rk30 = 1.0 / 3.0, rk31 = 2.0 / 3.0, rk32 = 2.0 / 3.0;
+        double E;
+        if (STAGE == 1) E = a.e0[i] + dt * LE;
+        else if (STAGE == 2) E = (rk20 * a.e0[i] + rk21 * a.es[i]) + (rk22 * dt) * LE;
+        else E = (rk30 * a.e0[i] + rk31 * a.es[i]) + (rk32 * dt) * LE;
+        // the conversion (utop_mx_cell)
+        auto U = [&](int q) -> double {
+            const double v = df_val(uh4[q], ul4[q]);
+            return FINAL ? v : v + (double)dn[q];
+        };
+        auto UB = [&](int q, int at) -> double {
+            const double v = df_val(a.uh[IBX + q][at], a.ul[IBX + q][at]);
+            return FINAL ? v : v + a.db[q][at];
+        };
+        const int off[3] = {1, b.SX, b.SX * b.SY};
+        double bcv[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double face = UB(q, i);
+            a.bf[q][i] = (float)face;
+            if (interior) {
+                bcv[q] = 0.5 * (face + UB(q, i - off[q]));
+                a.bc[q][i] = (float)bcv[q];
+            } else {
+                bcv[q] = a.bc[q][i];
+            }
+        }
+        const double bsq = (bcv[0] * bcv[0] + bcv[1] * bcv[1]) + bcv[2] * bcv[2];
+        const double rho = U(IRHO);
+        const double vx = U(IVX) / rho, vy = U(IVY) / rho, vz = U(IVZ) / rho;
+        const double vsq = (vx * vx + vy * vy) + vz * vz;
+        double e = (E - 0.5 * bsq) / rho - 0.5 * vsq;
+        double rn = rho;
+        bool changed = false;
+        if (interior) {
+            if (MODEL == 1) {
+                if (e < 0.0) { e = 0.0; changed = true; }
+            } else if (MODEL == 2 || MODEL == 3) {
+                if (rn < a.rho_floor) { rn = a.rho_floor; changed = true; }
+                if (e < a.eps_floor) { e = a.eps_floor; changed = true; }
+            }
+        }
+        if (changed) {  // FROMRVETOU after CUSTOM_CHECKRHO: re-derive U from the floored prims
+            const double un[4] = {rn, vx * rn, vy * rn, vz * rn};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (FINAL) {
+                    df_split(un[q], uh4[q], ul4[q]);
+                } else {
+                    dn[q] = (float)(un[q] - df_val(uh4[q], ul4[q]));
+                }
+            }
+            E = rn * (e + 0.5 * vsq) + 0.5 * bsq;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (FINAL) {
+                a.uh[q][i] = uh4[q];
+                a.ul[q][i] = ul4[q];
+            } else {
+                a.d[q][i] = dn[q];
+            }
+        }
+        if (FINAL) a.e0[i] = E;
+        else a.es[i] = E;
+        const double p = (rn * e) * (a.ggas - 1.0);
+        a.w[0][i] = (float)rn;
+        a.w[1][i] = (float)vx;
+        a.w[2][i] = (float)vy;
+        a.w[3][i] = (float)vz;
+        if (interior) {
+            a.w[4][i] = (float)p;
+            if (!(isfinite(p) && isfinite(vsq) && isfinite(rn))) atomicOr(a.flag, 1u);
+            if (fuse_dt)
+                dt_cell = cell_dt<COORD>(T, j, k, l, (double)(float)rn, (double)(float)p, (double)(float)vx,
+                                         (double)(float)vy, (double)(float)vz, (double)(float)bcv[0],
+                                         (double)(float)bcv[1], (double)(float)bcv[2], a.ggas, a.cfl);
+        }
+    }
     if (fuse_dt) block_min_dt(dt_cell, a.dtmin);
 }
 
@@ -477,6 +726,71 @@ void combine_model_mx(const Launcher& L, const Box& b, const Tabs& T, const Mixe
     }
 }
 
+CombineMx combine_args(const MixedBufs& m, const MixedParams& p) {
+    CombineMx a;
+    for (int q = 0; q < 8; ++q) { a.uh[q] = m.uh[q]; a.ul[q] = m.ul[q]; a.d[q] = m.d[q]; }
+    for (int q = 0; q < 3; ++q) a.db[q] = m.db[q];
+    a.e0 = m.e0;
+    a.es = m.es;
+    for (int q = 0; q < 5; ++q) a.w[q] = m.w[q];
+    for (int q = 0; q < 3; ++q) { a.bc[q] = m.bc[q]; a.ecorn[q] = m.E[q]; }
+    a.dt = m.dt;
+    a.geom_repeat = p.geom_repeat;
+    a.rho_floor = (float)p.rho_floor;
+    a.r_sh = (float)p.r_sh;
+    return a;
+}
+
+template <int COORD, int MODEL, int STAGE>
+void fused_tail_t(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>& pr, const FaceFluxT<float>* ff,
+                  const MixedBufs& m, const MixedParams& p, unsigned long long* dtmin) {
+    CtMx ct;
+    for (int q = 0; q < 3; ++q) {
+        ct.uh[q] = m.uh[IBX + q];
+        ct.ul[q] = m.ul[IBX + q];
+        ct.db[q] = m.db[q];
+    }
+    ct.dt = m.dt;
+    run(L, CUMC_K_CT, emf_ct_grid(b), EC_TX * EC_TY, sizeof(EmfCtSmemT<float>), k_emf_ct_mx<COORD, STAGE>, b, T, pr,
+        ff[0], ff[1], ff[2], ct);
+    UtopMx a = utop_args(m, p);
+    if (STAGE == 3 && dtmin) {  // the following iteration's finddt, fused (dtmin reset by the caller)
+        a.dtmin = dtmin;
+        a.cfl = p.cfl;
+    }
+    run(L, CUMC_K_COMBINE, g1((long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256), 256, 0,
+        k_combine_utop_mx<COORD, MODEL, STAGE>, b, T, ff[0], ff[1], ff[2], combine_args(m, p), a);
+}
+
+template <int COORD, int MODEL>
+void fused_tail_s(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>& pr, const FaceFluxT<float>* ff,
+                  const MixedBufs& m, const MixedParams& p, int stage, unsigned long long* dtmin) {
+    if (stage == 1) fused_tail_t<COORD, MODEL, 1>(L, b, T, pr, ff, m, p, dtmin);
+    else if (stage == 2) fused_tail_t<COORD, MODEL, 2>(L, b, T, pr, ff, m, p, dtmin);
+    else fused_tail_t<COORD, MODEL, 3>(L, b, T, pr, ff, m, p, dtmin);
+}
+
+template <int COORD>
+void fused_tail_c(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>& pr, const FaceFluxT<float>* ff,
+                  const MixedBufs& m, const MixedParams& p, int stage, unsigned long long* dtmin) {
+    switch (p.model) {
+        case 0: fused_tail_s<COORD, 0>(L, b, T, pr, ff, m, p, stage, dtmin); break;
+        case 1: fused_tail_s<COORD, 1>(L, b, T, pr, ff, m, p, stage, dtmin); break;
+        case 2: fused_tail_s<COORD, 2>(L, b, T, pr, ff, m, p, stage, dtmin); break;
+        default: fused_tail_s<COORD, 3>(L, b, T, pr, ff, m, p, stage, dtmin); break;
+    }
+}
+
+// the stage after the sweeps: k_emf_ct_mx, then k_combine_utop_mx
+void fused_tail(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>& pr, const FaceFluxT<float>* ff,
+                const MixedBufs& m, const MixedParams& p, int stage, unsigned long long* dtmin) {
+    switch (p.coord) {
+        case 1: fused_tail_c<1>(L, b, T, pr, ff, m, p, stage, dtmin); break;
+        case 2: fused_tail_c<2>(L, b, T, pr, ff, m, p, stage, dtmin); break;
+        default: fused_tail_c<3>(L, b, T, pr, ff, m, p, stage, dtmin); break;
+    }
+}
+
 }  // namespace
 
 cudaError_t mixed_attributes() {
@@ -502,6 +816,11 @@ void mixed_stage(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs
     FaceFluxT<float> ff[3];
     for (int d = 0; d < 3; ++d)
         for (int q = 0; q < 7; ++q) ff[d].f[q] = m.F[d][q];
+    if (p.fused) {
+        fused_tail(L, b, T, pr, ff, m, p, stage, dtmin);
+        boundary_mx(L, b, m, p);
+        return;
+    }
     EdgeET<float> ee;
     for (int q = 0; q < 3; ++q) ee.e[q] = m.E[q];
     run(L, 3, g1((long long)(b.nx + 1) * (b.ny + 1) * (b.nz + 1), 256), 256, 0, k_emf<float>, b, pr, ff[0], ff[1],

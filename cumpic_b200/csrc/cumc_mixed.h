@@ -39,6 +39,8 @@ struct MixedParams {
     signed char fac[6][8];
     int model, coord, recon, geom_repeat;
     int sm_count;  // multiprocessors of the device (grid sizing)
+    int fused = 1; // the stage's tiled EMF + CT and fused combine + conversion kernels
+                   // (0: k_emf, k_combine_mx, k_utop_mx)
 };
 
 // How the mixed kernels are launched: the caller's stream, and hooks that

@@ -89,3 +89,35 @@ def test_curvilinear_mixed_vs_fp64(make):
     assert np.all(np.isfinite(db["cons"][3:-3, 3:-3, 3:-3]))
     rel = rel_l1_interior(db, a.download())
     assert rel[0] <= RHO_L1_TOL, rel
+
+
+def test_fused_stage_equals_split(monkeypatch):
+    """the default mixed stage (tiled EMF + CT, combine fused with the
+    conversions) agrees with the split one (k_emf, k_combine_mx, k_utop_mx)
+    on a Cartesian box and on a torus with floors. Both evaluate the same
+    expressions, but the mixed unit contracts to FMA and may pair a product
+    with a different sum in the two forms, so they agree to FP32 round-off
+    rather than bit for bit."""
+    from cumpic_b200.solver import CUMC3D
+    out = {}
+    for mode in (None, "split"):
+        if mode:
+            monkeypatch.setenv("CUMC_MX_STAGE", mode)
+        else:
+            monkeypatch.delenv("CUMC_MX_STAGE", raising=False)
+        for name, prob in (("ot", P.orszag_tang(37, ny=29, nz=40)), ("torus", P.torus(24, 16, 40))):
+            prob.precision = N.MIXED
+            s = CUMC3D(prob)
+            s.upload()
+            s.initial_update()
+            s.advance(4)
+            out[(mode, name)] = s.download()
+            s.close()
+    for name in ("ot", "torus"):
+        a, b = out[(None, name)], out[("split", name)]
+        rel = rel_l1_interior(a, b)
+        assert max(rel.values()) <= 1.0e-6, (name, rel)
+        x, y = a["cons"][3:-3, 3:-3, 3:-3], b["cons"][3:-3, 3:-3, 3:-3]
+        for q in range(8):
+            scale = np.max(np.abs(y[..., q])) or 1.0
+            assert np.max(np.abs(x[..., q] - y[..., q])) <= 1.0e-5 * scale, (name, q)
