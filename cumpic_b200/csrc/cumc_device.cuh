@@ -368,4 +368,128 @@ __device__ __forceinline__ void geom_ct(const Tabs& T, int j, int k, int l, CTf&
     }
 }
 
+// ---------------------------------------------------------------------------
+// HLL of the mixed form (float states). The wave speeds and the two stored
+// tangential-field components are formed in FP32, in the reciprocal form of
+// hll_flux7 (five divisors, each reciprocal formed once); the five hydro
+// components (rho, rho v, E) take their side fluxes, conserved values and HLL
+// combination in FP64 from the FP32 states, with each side's internal energy,
+// E, B^2/2 and v.B in FP64. Measured on Orszag-Tang 256^3 to t = 0.5, the
+// all-FP32 form leaves the density 1.06e-5 (relative L1) from the FP64 run,
+// this form 8.0e-6: the side fluxes' and the combination's FP32 rounding is
+// the largest error left once the states are FP32.
+//
+// The FP64 quotients (by rho, by gamma-1, by sR-sL) start from the FP32
+// reciprocal and take one Newton-Raphson step for 1/x, r' = r (2 - x r),
+// which squares its relative error (6e-8 -> ~4e-15): FP64 accuracy without
+// an FP64 division.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double rcp_newton(double x, float r0) {
+    const double r = (double)r0;
+    return r * (2.0 - x * r);
+}
+
+// one side's flux (F) or conserved value (U) of component q, in T from the
+// FP32 side primitives and the side's derived scalars
+template <typename T, int DIR>
+__device__ __forceinline__ T side_f(const FaceSide<DIR, float>& s, int q, double Ex, double hb2x, double vdotbx) {
+    constexpr int t1 = (DIR + 1) % 3, t2 = (DIR + 2) % 3;
+    const T rho = s.rho, vn = s.v[DIR], bn = s.b[DIR], p = s.p, hb2 = (T)hb2x, E = (T)Ex, vdotb = (T)vdotbx;
+    if (q == IRHO) return rho * vn;
+    if (q == IVX + DIR) return ((vn * rho * vn + p) + hb2) - bn * bn;
+    if (q == IVX + t1) return (T)s.v[t1] * rho * vn - bn * (T)s.b[t1];
+    if (q == IVX + t2) return (T)s.v[t2] * rho * vn - bn * (T)s.b[t2];
+    if (q == ITAU) return (E * vn + (p + hb2) * vn) - bn * vdotb;
+    if (q == IBX + t1) return vn * (T)s.b[t1] - (T)s.v[t1] * bn;
+    return vn * (T)s.b[t2] - (T)s.v[t2] * bn;
+}
+template <typename T, int DIR>
+__device__ __forceinline__ T side_u(const FaceSide<DIR, float>& s, int q, double Ex) {
+    return q == IRHO ? (T)s.rho : q <= IVZ ? (T)s.v[q - IVX] * (T)s.rho : q == ITAU ? (T)Ex : (T)s.b[q - IBX];
+}
+
+// a side's internal energy, E, B^2/2 and v.B in FP64 from its FP32 primitives
+// (the FaceSide expressions); irho32, ig32: FP32 reciprocals of rho and gamma-1
+struct SideScalars {
+    double E, hb2, vdotb;
+};
+__device__ __forceinline__ SideScalars side_scalars64(const float (&w)[8], float irho32, double ig) {
+    const double rho = w[IRHO], vx = w[IVX], vy = w[IVY], vz = w[IVZ], bx = w[IBX], by = w[IBY], bz = w[IBZ];
+    const double e = (double)w[ITAU] * rcp_newton(rho, irho32) * ig;
+    const double vsq = (vx * vx + vy * vy) + vz * vz, bsq = (bx * bx + by * by) + bz * bz;
+    return {rho * (e + 0.5 * vsq) + 0.5 * bsq, 0.5 * bsq, (bx * vx + by * vy) + bz * vz};
+}
+
+template <int DIR>
+__device__ __forceinline__ void hll_flux7_mixed(const float (&wl)[8], const float (&wr)[8], float ggas,
+                                                float (&out)[7]) {
+    constexpr int ivn = IVX + DIR;
+    constexpr int ibn = IBX + DIR, ibt1 = IBX + (DIR + 1) % 3, ibt2 = IBX + (DIR + 2) % 3;
+    constexpr int HYDRO = 5;  // components 0..4 in FP64
+    const float irL = 1.0f / wl[IRHO], irR = 1.0f / wr[IRHO];
+    float sL, sR;
+    {
+        const float csL = sqrtf((ggas * wl[ITAU]) * irL);
+        const float csR = sqrtf((ggas * wr[ITAU]) * irR);
+        const float cfsL = signalspeed_recip<float>(csL, wl[ibn], wl[ibt1], wl[ibt2], irL);
+        const float cfsR = signalspeed_recip<float>(csR, wr[ibn], wr[ibt1], wr[ibt2], irR);
+        const float sqL = sqrtf(wl[IRHO]), sqR = sqrtf(wr[IRHO]);
+        const float isq = 1.0f / (sqL + sqR);
+        const float ubar = (sqL * wl[ivn] + sqR * wr[ivn]) * isq;
+        const float cbar = (sqL * cfsL + sqR * cfsR) * isq;
+        sL = fminf(wl[ivn] - cfsL, ubar - cbar);
+        sR = fmaxf(wr[ivn] + cfsR, ubar + cbar);
+    }
+    using Side = FaceSide<DIR, float>;
+    const float ig = 1.0f / (ggas - 1.0f);
+    const double igd = rcp_newton((double)ggas - 1.0, ig);
+    const SideScalars aL = side_scalars64(wl, irL, igd), aR = side_scalars64(wr, irR, igd);
+    // the FP32 side (tangential-field components only read rho, v, b)
+    const Side L(wl, wl[ITAU] * irL * ig, typename Side::GivenEps{});
+    const Side Rs(wr, wr[ITAU] * irR * ig, typename Side::GivenEps{});
+    constexpr int bt_a = DIR == 0 ? IBY : IBX;
+    constexpr int bt_b = DIR == 2 ? IBY : IBZ;
+    const int comp[7] = {IRHO, IVX, IVY, IVZ, ITAU, bt_a, bt_b};
+    if (sL >= 0.0f) {
+#pragma unroll
+        for (int q = 0; q < 7; ++q)
+            out[q] = q < HYDRO ? (float)side_f<double>(L, comp[q], aL.E, aL.hb2, aL.vdotb) : L.f(comp[q]);
+    } else if (sR >= 0.0f) {
+        const float idsf = 1.0f / (sR - sL), lrf = sL * sR;
+        const double cl = sL, cr = sR, ids = rcp_newton(cr - cl, idsf), lr = cl * cr;
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            if (q < HYDRO) {
+                const double yl = side_f<double>(L, comp[q], aL.E, aL.hb2, aL.vdotb);
+                const double yr = side_f<double>(Rs, comp[q], aR.E, aR.hb2, aR.vdotb);
+                const double xl = side_u<double>(L, comp[q], aL.E), xr = side_u<double>(Rs, comp[q], aR.E);
+                out[q] = (float)(((cr * yl - cl * yr) + lr * (xr - xl)) * ids);
+            } else {
+                const float yl = L.f(comp[q]), yr = Rs.f(comp[q]), xl = L.u(comp[q]), xr = Rs.u(comp[q]);
+                out[q] = ((sR * yl - sL * yr) + lrf * (xr - xl)) * idsf;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 7; ++q)
+            out[q] = q < HYDRO ? (float)side_f<double>(Rs, comp[q], aR.E, aR.hb2, aR.vdotb) : Rs.f(comp[q]);
+    }
+}
+
+// the sweeps' HLL solve: hll_flux7 in FP64; hll_flux7_mixed for the mixed
+// form's float states (a mixed-unit build with CUMC_MX_HLL_FP32 defined takes
+// the all-FP32 reciprocal form instead: faster, 1.06e-5 above)
+template <int DIR, typename R, bool RECIP>
+__device__ __forceinline__ void sweep_hll(const R (&wl)[8], const R (&wr)[8], R ggas, R (&fx)[7]) {
+    if constexpr (sizeof(R) == 4) {
+#ifdef CUMC_MX_HLL_FP32
+        hll_flux7<DIR, R, true>(wl, wr, ggas, fx);
+#else
+        hll_flux7_mixed<DIR>(wl, wr, ggas, fx);
+#endif
+    } else {
+        hll_flux7<DIR, R, RECIP>(wl, wr, ggas, fx);
+    }
+}
+
 }  // namespace cumc

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(128) k_sweep(Box b, Tabs T, PrimT<R> pr, R gga
     wr[IBX + DIR] = bn;
 
     R fx[7];
-    hll_flux7<DIR>(wl, wr, ggas, fx);
+    sweep_hll<DIR, R, false>(wl, wr, ggas, fx);
 #pragma unroll
     for (int i = 0; i < 7; ++i) out.f[i][base] = fx[i];
 }

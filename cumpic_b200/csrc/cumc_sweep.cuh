@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(SW_THREADS, 2) k_sweep_tile(Box b, Tabs T, Pri
     wl[IBX + DIR] = bn;
     wr[IBX + DIR] = bn;
     R fx[7];
-    hll_flux7<DIR>(wl, wr, ggas, fx);
+    sweep_hll<DIR, R, false>(wl, wr, ggas, fx);
 #pragma unroll
     for (int i = 0; i < 7; ++i) out.f[i][gi] = fx[i];
 }
