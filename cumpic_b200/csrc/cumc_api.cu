@@ -353,11 +353,14 @@ void combine_stage(cumc_ctx* c, const Box& b, const Prim& pr, const FaceFlux* ff
         return;
     }
     constexpr int S = STAGE == 0 ? 1 : STAGE;
-    if (c->emf_tiles)
-        launch_grid(c, CUMC_K_CT, emf_ct_grid(b), EC_TX * EC_TY, sizeof(EmfCtSmem), k_emf_ct<COORD, S>, b, c->tabs, pr,
-                    ff[0], ff[1], ff[2], a);
-    else
+    if (c->emf_tiles) {
+        int seg;
+        const dim3 g = emf_ct_grid(b, (long long)c->sm_count * CUMC_EC_MINB, &seg);
+        launch_grid(c, CUMC_K_CT, g, EC_TX * EC_TY, sizeof(EmfCtSmem), k_emf_ct<COORD, S>, b, c->tabs, pr, ff[0], ff[1],
+                    ff[2], a, seg);
+    } else {
         launch(c, CUMC_K_CT, n, 256, k_ct<COORD, S>, b, c->tabs, a);
+    }
     if (c->pair_combine && pairs_aligned<S>(b, ff, a, o)) {
         const long long np = (long long)((b.nx + 2) / 2) * (b.ny + 1) * (b.nz + 1);
         launch(c, CUMC_K_COMBINE, np, 256, k_combine_utop2<COORD, MODEL, S>, b, c->tabs, pr, ff[0], ff[1], ff[2], a,

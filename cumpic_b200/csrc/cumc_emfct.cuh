@@ -23,7 +23,7 @@ namespace cumc {
 constexpr int EC_TX = 32, EC_TY = 8;           // face triples of a tile
 constexpr int EC_CX = EC_TX + 2, EC_CY = EC_TY + 2;  // cells j0-1..j0+32, k0-1..k0+8
 constexpr int EC_EX = EC_TX + 1, EC_EY = EC_TY + 1;  // edges j0-1..j0+31, k0-1..k0+7
-constexpr int EC_SEG = 32;                     // planes a block marches over
+constexpr int EC_SEG = 32;                     // planes a block marches over (at most; emf_ct_grid)
 
 // shared memory of a tile; R is the EMFs' type (double, or float in the
 // mixed form)
@@ -157,14 +157,15 @@ __device__ __forceinline__ void ec_edge_finish(const Box& b, EmfCtSmemT<R>& S, c
 #endif
 template <int COORD, int STAGE>
 __global__ void __launch_bounds__(EC_TX * EC_TY, CUMC_EC_MINB) k_emf_ct(Box b, Tabs T, Prim pr, FaceFlux fx,
-                                                                      FaceFlux fy, FaceFlux fz, CombineArgs a) {
+                                                                      FaceFlux fy, FaceFlux fz, CombineArgs a,
+                                                                      int seg) {
     extern __shared__ __align__(16) unsigned char ec_raw[];
     EmfCtSmem& S = *reinterpret_cast<EmfCtSmem*>(ec_raw);
     if (b.skip && *b.skip) return;
     constexpr int NE = EC_EX * EC_EY, NT = EC_TX * EC_TY;
     static_assert(NE > NT && NE <= 2 * NT, "two edges a thread at most");
     const int j0 = blockIdx.x * EC_TX, k0 = blockIdx.y * EC_TY;
-    const int l0 = blockIdx.z * EC_SEG, l1 = min(l0 + EC_SEG, b.nz + 1);
+    const int l0 = blockIdx.z * seg, l1 = min(l0 + seg, b.nz + 1);
     const int tj = threadIdx.x % EC_TX, tk = threadIdx.x / EC_TX;
     const int j = j0 + tj, k = k0 + tk;
     const bool mine = j <= b.nx && k <= b.ny;
@@ -217,9 +218,16 @@ __global__ void __launch_bounds__(EC_TX * EC_TY, CUMC_EC_MINB) k_emf_ct(Box b, T
     }
 }
 
-inline dim3 emf_ct_grid(const Box& b) {
-    return dim3((unsigned)((b.nx + 1 + EC_TX - 1) / EC_TX), (unsigned)((b.ny + 1 + EC_TY - 1) / EC_TY),
-                (unsigned)((b.nz + 1 + EC_SEG - 1) / EC_SEG));
+// grid of a tiled EMF + CT launch and the planes a block marches over: 32,
+// halved (down to 4) while the grid would not fill `slots` resident blocks
+// twice (small boxes: the 128^3 adjoint box, the torus); each segment repeats
+// one plane of cell and edge EMFs
+inline dim3 emf_ct_grid(const Box& b, long long slots, int* seg) {
+    const unsigned gx = (unsigned)((b.nx + 1 + EC_TX - 1) / EC_TX), gy = (unsigned)((b.ny + 1 + EC_TY - 1) / EC_TY);
+    int s = EC_SEG;
+    while (s > 4 && (long long)gx * gy * ((b.nz + 1 + s - 1) / s) < 2 * slots) s /= 2;
+    *seg = s;
+    return dim3(gx, gy, (unsigned)((b.nz + 1 + s - 1) / s));
 }
 
 }  // namespace cumc

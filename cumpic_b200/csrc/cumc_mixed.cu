@@ -242,13 +242,14 @@ struct CtMx {
 #endif
 template <int COORD, int STAGE>
 __global__ void __launch_bounds__(EC_TX * EC_TY, CUMC_ECMX_MINB) k_emf_ct_mx(Box b, Tabs T, PrimT<float> pr, FaceFluxT<float> fx,
-                                                               FaceFluxT<float> fy, FaceFluxT<float> fz, CtMx a) {
+                                                               FaceFluxT<float> fy, FaceFluxT<float> fz, CtMx a,
+                                                               int seg) {
     extern __shared__ __align__(16) unsigned char ecm_raw[];
     EmfCtSmemT<float>& S = *reinterpret_cast<EmfCtSmemT<float>*>(ecm_raw);
     if (b.skip && *b.skip) return;
     constexpr int NE = EC_EX * EC_EY, NT = EC_TX * EC_TY;
     const int j0 = blockIdx.x * EC_TX, k0 = blockIdx.y * EC_TY;
-    const int l0 = blockIdx.z * EC_SEG, l1 = min(l0 + EC_SEG, b.nz + 1);
+    const int l0 = blockIdx.z * seg, l1 = min(l0 + seg, b.nz + 1);
     const int tj = threadIdx.x % EC_TX, tk = threadIdx.x / EC_TX;
     const int j = j0 + tj, k = k0 + tk;
     const bool mine = j <= b.nx && k <= b.ny;
@@ -751,8 +752,10 @@ void fused_tail_t(const Launcher& L, const Box& b, const Tabs& T, const PrimT<fl
         ct.db[q] = m.db[q];
     }
     ct.dt = m.dt;
-    run(L, CUMC_K_CT, emf_ct_grid(b), EC_TX * EC_TY, sizeof(EmfCtSmemT<float>), k_emf_ct_mx<COORD, STAGE>, b, T, pr,
-        ff[0], ff[1], ff[2], ct);
+    int seg;
+    const dim3 g = emf_ct_grid(b, (long long)p.sm_count * CUMC_ECMX_MINB, &seg);
+    run(L, CUMC_K_CT, g, EC_TX * EC_TY, sizeof(EmfCtSmemT<float>), k_emf_ct_mx<COORD, STAGE>, b, T, pr, ff[0], ff[1],
+        ff[2], ct, seg);
     UtopMx a = utop_args(m, p);
     if (STAGE == 3 && dtmin) {  // the following iteration's finddt, fused (dtmin reset by the caller)
         a.dtmin = dtmin;
