@@ -33,7 +33,7 @@ constexpr int WK_THREADS = 64;
 // resident blocks per SM the walker and the x sweep are compiled for (the
 // register budget a thread gets); build-time tunables
 #ifndef CUMC_WALK_MINB
-#define CUMC_WALK_MINB 8
+#define CUMC_WALK_MINB 9
 #endif
 #ifndef CUMC_XWARP_MINB
 #define CUMC_XWARP_MINB 8
