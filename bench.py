@@ -395,11 +395,51 @@ def mixed_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> d
             relp = rel_l1_interior(s.download(), res[NN.FP64][0])
             s.close()
             out["fp64_perturbed_1e-12_rel_l1_at_t_end"] = {k: relp[q] for q, k in enumerate(names)}
+            out["hll_fp32"] = mixed_fp32_form(n, steps, warmup, fp64_ms_per_step, res[NN.FP64][0], prob.t_end)
         out["vs_fp64"][f"bscale_{bscale:g}"] = {"rel_l1": {k: rel[q] for q, k in enumerate(names)},
                                                 "max_divb_norm": res[NN.MIXED][1],
                                                 "max_divb_norm_fp64": res[NN.FP64][1],
                                                 "steps": {"fp64": res[NN.FP64][2], "mixed": res[NN.MIXED][2]}}
     return out
+
+
+def mixed_fp32_form(n: int, steps: int, warmup: int, fp64_ms_per_step: float, fp64_state: dict,
+                    t_end: float) -> dict:
+    """The mixed form with its HLL solve all in FP32 (CUMC_MX_HLL=fp32, the
+    reciprocal form): throughput and the density error at t_end against the
+    FP64 run."""
+    import torch
+    from cumpic_b200 import _native as NN
+    from cumpic_b200 import problems as P
+    from cumpic_b200.solver import CUMC3D
+    from compare import rel_l1_interior
+    os.environ["CUMC_MX_HLL"] = "fp32"
+    try:
+        sim = CUMC3D(P.orszag_tang(n, precision=NN.MIXED))
+        sim.upload()
+        sim.initial_update()
+        stream = torch.cuda.ExternalStream(sim.stream_handle())
+        sim.advance(warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.advance(steps)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        sim.close()
+        s = CUMC3D(P.orszag_tang(n, precision=NN.MIXED))
+        s.upload()
+        s.initial_update()
+        s.run(t_end)
+        rel = rel_l1_interior(s.download(), fp64_state)
+        s.close()
+    finally:
+        os.environ.pop("CUMC_MX_HLL", None)
+    return {"value": n ** 3 * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
+            "speedup_vs_fp64": fp64_ms_per_step / (ms / steps), "accuracy_t": t_end, "rel_l1_rho": rel[0],
+            "what": "CUMC_MX_HLL=fp32: the HLL solve all in FP32 (reciprocal form) instead of its hydro components "
+                    "combined in FP64"}
 
 
 def fast_section(n: int, steps: int, warmup: int, fp64_ms_per_step: float) -> dict:

@@ -1173,6 +1173,8 @@ int cumc_init(const cumc_config* cfg, cumc_ctx** out) {
         mp.sm_count = c->sm_count;
         const char* ms = getenv("CUMC_MX_STAGE");
         mp.fused = !(ms && std::strcmp(ms, "split") == 0);
+        const char* mh = getenv("CUMC_MX_HLL");
+        mp.hll_fp32 = mh && std::strcmp(mh, "fp32") == 0;
     }
     if ((rc = dalloc(c, &c->dsoa, 8)) != CUMC_OK) return fail_init(rc);
     if ((rc = dalloc(c, &c->scal, 4)) != CUMC_OK) return fail_init(rc);

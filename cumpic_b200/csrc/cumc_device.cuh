@@ -476,17 +476,15 @@ __device__ __forceinline__ void hll_flux7_mixed(const float (&wl)[8], const floa
     }
 }
 
-// the sweeps' HLL solve: hll_flux7 in FP64; hll_flux7_mixed for the mixed
-// form's float states (a mixed-unit build with CUMC_MX_HLL_FP32 defined takes
-// the all-FP32 reciprocal form instead: faster, 1.06e-5 above)
+// the sweeps' HLL solve: hll_flux7 in FP64 (RECIP: the CUMC_FP64_FAST form).
+// For the mixed form's float states, RECIP selects the all-FP32 reciprocal
+// form of hll_flux7 (faster; density 1.06e-5 from the FP64 run at t_end above)
+// and its absence hll_flux7_mixed (the default).
 template <int DIR, typename R, bool RECIP>
 __device__ __forceinline__ void sweep_hll(const R (&wl)[8], const R (&wr)[8], R ggas, R (&fx)[7]) {
     if constexpr (sizeof(R) == 4) {
-#ifdef CUMC_MX_HLL_FP32
-        hll_flux7<DIR, R, true>(wl, wr, ggas, fx);
-#else
-        hll_flux7_mixed<DIR>(wl, wr, ggas, fx);
-#endif
+        if constexpr (RECIP) hll_flux7<DIR, R, true>(wl, wr, ggas, fx);
+        else hll_flux7_mixed<DIR>(wl, wr, ggas, fx);
     } else {
         hll_flux7<DIR, R, RECIP>(wl, wr, ggas, fx);
     }

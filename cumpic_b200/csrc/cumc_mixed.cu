@@ -642,23 +642,33 @@ __global__ void __launch_bounds__(256) k_export_mx(Box b, UtopMx a, double* __re
 
 template <int DIR>
 void sweep_mx(const Launcher& L, const Box& b, const Tabs& T, const PrimT<float>& pr, float ggas, const MixedBufs& m,
-              int recon, int sm_count) {
+              int recon, int sm_count, bool fp32) {
     FaceFluxT<float> out;
     for (int q = 0; q < 7; ++q) out.f[q] = m.F[DIR][q];
+    const bool ppm = recon == 4;
     if (DIR > 0) {  // column walker along y or z, window in shared memory
         constexpr int D = DIR > 0 ? DIR : 1;
         int nseg;
         const int seg = walk_segment_for<D>(b, WalkGeom<D>::ncols(b), sm_count, &nseg);
         const dim3 grid((unsigned)((WalkGeom<D>::ncols(b) + WK_THREADS - 1) / WK_THREADS), (unsigned)nseg);
         const size_t sm = walk_smem<float>(D);
-        if (recon == 4) run(L, DIR, grid, WK_THREADS, sm, k_sweep_walk_sm<D, 4, float>, b, T, pr, ggas, out, seg, out, 0, -1);
-        else run(L, DIR, grid, WK_THREADS, sm, k_sweep_walk_sm<D, 1, float>, b, T, pr, ggas, out, seg, out, 0, -1);
+        if (fp32)
+            run(L, DIR, grid, WK_THREADS, sm,
+                ppm ? k_sweep_walk_sm<D, 4, float, false, true> : k_sweep_walk_sm<D, 1, float, false, true>, b, T, pr,
+                ggas, out, seg, out, 0, -1);
+        else
+            run(L, DIR, grid, WK_THREADS, sm, ppm ? k_sweep_walk_sm<D, 4, float> : k_sweep_walk_sm<D, 1, float>, b, T,
+                pr, ggas, out, seg, out, 0, -1);
         return;
     }
     // x: one lane per cell
     const long long n = xwarp_threads(b);
-    if (recon == 4) run(L, DIR, g1(n, 128), 128, 0, k_sweep_xwarp<4, float>, b, T, pr, ggas, out, out, 0, -1);
-    else run(L, DIR, g1(n, 128), 128, 0, k_sweep_xwarp<1, float>, b, T, pr, ggas, out, out, 0, -1);
+    if (fp32)
+        run(L, DIR, g1(n, 128), 128, 0, ppm ? k_sweep_xwarp<4, float, false, true> : k_sweep_xwarp<1, float, false, true>,
+            b, T, pr, ggas, out, out, 0, -1);
+    else
+        run(L, DIR, g1(n, 128), 128, 0, ppm ? k_sweep_xwarp<4, float> : k_sweep_xwarp<1, float>, b, T, pr, ggas, out,
+            out, 0, -1);
 }
 
 UtopMx utop_args(const MixedBufs& m, const MixedParams& p) {
@@ -813,9 +823,9 @@ void mixed_stage(const Launcher& L, const Box& b, const Tabs& T, const MixedBufs
     for (int q = 0; q < 5; ++q) pr.w[q] = m.w[q];
     for (int q = 0; q < 3; ++q) { pr.bc[q] = m.bc[q]; pr.bf[q] = m.bf[q]; }
     const float ggas = (float)p.ggas;
-    sweep_mx<0>(L, b, T, pr, ggas, m, p.recon, p.sm_count);
-    sweep_mx<1>(L, b, T, pr, ggas, m, p.recon, p.sm_count);
-    sweep_mx<2>(L, b, T, pr, ggas, m, p.recon, p.sm_count);
+    sweep_mx<0>(L, b, T, pr, ggas, m, p.recon, p.sm_count, p.hll_fp32 != 0);
+    sweep_mx<1>(L, b, T, pr, ggas, m, p.recon, p.sm_count, p.hll_fp32 != 0);
+    sweep_mx<2>(L, b, T, pr, ggas, m, p.recon, p.sm_count, p.hll_fp32 != 0);
     FaceFluxT<float> ff[3];
     for (int d = 0; d < 3; ++d)
         for (int q = 0; q < 7; ++q) ff[d].f[q] = m.F[d][q];

@@ -41,6 +41,8 @@ struct MixedParams {
     int sm_count;  // multiprocessors of the device (grid sizing)
     int fused = 1; // the stage's tiled EMF + CT and fused combine + conversion kernels
                    // (0: k_emf, k_combine_mx, k_utop_mx)
+    int hll_fp32 = 0;  // the HLL solve all in FP32 (reciprocal form) instead of
+                       // the hydro components in FP64 (hll_flux7_mixed)
 };
 
 // How the mixed kernels are launched: the caller's stream, and hooks that

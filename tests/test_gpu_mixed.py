@@ -121,3 +121,18 @@ def test_fused_stage_equals_split(monkeypatch):
         for q in range(8):
             scale = np.max(np.abs(y[..., q])) or 1.0
             assert np.max(np.abs(x[..., q] - y[..., q])) <= 1.0e-5 * scale, (name, q)
+
+
+def test_fp32_hll_form(monkeypatch):
+    """CUMC_MX_HLL=fp32 (the HLL solve all in FP32) runs the same problem
+    within the bar, and is a different arithmetic from the default form,
+    whose hydro HLL components are combined in FP64"""
+    a = _run(P.orszag_tang(32), N.FP64, t_end=0.05)
+    ref = a.download()
+    b = _run(P.orszag_tang(32), N.MIXED, t_end=0.05)
+    monkeypatch.setenv("CUMC_MX_HLL", "fp32")
+    c = _run(P.orszag_tang(32), N.MIXED, t_end=0.05)
+    db, dc = b.download(), c.download()
+    rel_c = rel_l1_interior(dc, ref)
+    assert rel_c[0] <= RHO_L1_TOL, rel_c
+    assert not np.array_equal(db["cons"], dc["cons"])
