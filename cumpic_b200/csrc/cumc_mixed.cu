@@ -58,6 +58,17 @@ __device__ __forceinline__ void df_split(double v, float& hi, float& lo) {
 }
 __device__ __forceinline__ double df_val(float hi, float lo) { return (double)hi + (double)lo; }
 
+// x / y in FP64 through the FP32 reciprocal of y and one Newton-Raphson step
+// (rcp_newton): a few units in the last place, without an FP64 division
+// (CUMC_MX_RCP; otherwise the IEEE quotient)
+__device__ __forceinline__ double qdiv(double x, double y) {
+#ifdef CUMC_MX_RCP
+    return x * rcp_newton(y, 1.0f / (float)y);
+#else
+    return x / y;
+#endif
+}
+
 template <typename K, typename... Args>
 void run(const Launcher& L, int cls, dim3 grid, int block, size_t smem, K kern, Args... args) {
     if (grid.x == 0 || grid.y == 0 || grid.z == 0) return;
@@ -291,9 +302,12 @@ __global__ void __launch_bounds__(EC_TX * EC_TY, CUMC_ECMX_MINB) k_emf_ct_mx(Box
             CTf g;
             geom_ct<COORD>(T, j, k, l, g);
             double LB[3];
-            LB[0] = -((Ez * g.bx_ez_p - Ez_km * g.bx_ez_m) / g.bx_ez_c - (Ey * g.bx_ey_p - Ey_lm * g.bx_ey_m) / g.bx_ey_c);
-            LB[1] = -((Ex * g.by_ex_p - Ex_lm * g.by_ex_m) / g.by_ex_c - (Ez * g.by_ez_p - Ez_jm * g.by_ez_m) / g.by_ez_c);
-            LB[2] = -((Ey * g.bz_ey_p - Ey_jm * g.bz_ey_m) / g.bz_ey_c - (Ex * g.bz_ex_p - Ex_km * g.bz_ex_m) / g.bz_ex_c);
+            LB[0] = -(qdiv(Ez * g.bx_ez_p - Ez_km * g.bx_ez_m, g.bx_ez_c) -
+                      qdiv(Ey * g.bx_ey_p - Ey_lm * g.bx_ey_m, g.bx_ey_c));
+            LB[1] = -(qdiv(Ex * g.by_ex_p - Ex_lm * g.by_ex_m, g.by_ex_c) -
+                      qdiv(Ez * g.by_ez_p - Ez_jm * g.by_ez_m, g.by_ez_c));
+            LB[2] = -(qdiv(Ey * g.bz_ey_p - Ey_jm * g.bz_ey_m, g.bz_ey_c) -
+                      qdiv(Ex * g.bz_ex_p - Ex_km * g.bz_ex_m, g.bz_ex_c));
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 if (STAGE == 1) {
@@ -504,9 +518,9 @@ __global__ void __launch_bounds__(256, CUMC_CUMX_MINB) k_combine_utop_mx(Box b, 
         }
         const double bsq = (bcv[0] * bcv[0] + bcv[1] * bcv[1]) + bcv[2] * bcv[2];
         const double rho = U(IRHO);
-        const double vx = U(IVX) / rho, vy = U(IVY) / rho, vz = U(IVZ) / rho;
+        const double vx = qdiv(U(IVX), rho), vy = qdiv(U(IVY), rho), vz = qdiv(U(IVZ), rho);
         const double vsq = (vx * vx + vy * vy) + vz * vz;
-        double e = (E - 0.5 * bsq) / rho - 0.5 * vsq;
+        double e = qdiv(E - 0.5 * bsq, rho) - 0.5 * vsq;
         double rn = rho;
         bool changed = false;
         if (interior) {
