@@ -59,13 +59,15 @@ __device__ __forceinline__ void df_split(double v, float& hi, float& lo) {
 __device__ __forceinline__ double df_val(float hi, float lo) { return (double)hi + (double)lo; }
 
 // x / y in FP64 through the FP32 reciprocal of y and one Newton-Raphson step
-// (rcp_newton): a few units in the last place, without an FP64 division
-// (CUMC_MX_RCP; otherwise the IEEE quotient)
+// for 1/y (rcp_newton): within a few units in the last place of the IEEE
+// quotient, without an FP64 division. The fused stage's CT curl and its
+// conversions use it (0.90 -> 0.84 ms and 0.59 -> 0.54 ms a stage at 256^3);
+// a build with CUMC_MX_IEEE_DIV defined takes the IEEE quotient instead.
 __device__ __forceinline__ double qdiv(double x, double y) {
-#ifdef CUMC_MX_RCP
-    return x * rcp_newton(y, 1.0f / (float)y);
-#else
+#ifdef CUMC_MX_IEEE_DIV
     return x / y;
+#else
+    return x * rcp_newton(y, 1.0f / (float)y);
 #endif
 }
 
