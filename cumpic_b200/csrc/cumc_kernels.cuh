@@ -771,11 +771,13 @@ __global__ void __launch_bounds__(256) k_boundary(Box b, BoundArgsT<R> a) {
         l = r / b.SX + 1;
         j = r % b.SX - 2;
     } else if ((t -= ysl) < xsl) {
-        const int s = (int)(t / ((long long)b.ny * b.nz));
-        const int r = (int)(t % ((long long)b.ny * b.nz));
+        // the six x ghosts of a row on six consecutive threads, so that a warp
+        // reads and writes a few row segments instead of 32 rows
+        const int s = (int)(t % 6);
+        const long long r = t / 6;
         j = s < 3 ? s - 2 : b.nx + s - 2;
-        l = r / b.ny + 1;
-        k = r % b.ny + 1;
+        l = (int)(r / b.ny) + 1;
+        k = (int)(r % b.ny) + 1;
     } else {
         return;
     }
